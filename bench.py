@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the libMeshlessVis hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c3] [--form auto|plain|tensor]
+
+One step = one pass of the hot path over one particle set resident in HBM:
+the 3D half-spectrum Fourier sum of every group, then slice extraction and
+batched 2D C2R of all the workload's views.  Default workload: C2 (N=262,144
+Plummer particles, 32-NN weights and radii, Wendland D3 C2, 128x128x65
+half-spectrum, 64 views rotating about y, 128^2 images).
+
+Prints one JSON line (rank 0).  value = particle x frequency terms per second
+over the whole step (GTerms/s), device time by CUDA events on the library's
+stream, max over ranks.  e2e = the same metric through the public C API with
+host buffers: registration (H2D of the particles from pinned memory),
+spectrum, views and D2H of the images, every step.
+
+Multi-GPU: the path does not shard on one particle set here, so N GPUs run N
+independent replicas (weak scaling); value sums all ranks' terms.
+--impl reference times the reference's own CPU implementation
+(oracle/_ref, built from the reference sources; the FP64 oracle's C code if
+that is absent) on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FP32_LANES_PER_SM = 128
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["c1", "c2", "c3"], default="c2")
+    p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from libmeshlessvis_b200 import workloads as W
+
+    if name == "c1":
+        return W.c1()
+    if name == "c3":
+        return W.c3()
+    return W.c2()
+
+
+def terms_per_step(w):
+    kx, ky, kz = w["grid"]
+    g = kx * ky * (kz // 2 + 1)
+    n = sum(len(c) for c, _, _ in w["groups"])
+    return n * g, n, g
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = [ln.split(", ") for ln in Path(self.f.name).read_text().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) >= 9:
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline(w, sample_cutoff=(64, 64)):
+    """The reference's own fourier_transform (OpenMP, all host threads) on the
+    workload's particles, for one slice of 2*cx*cy frequencies."""
+    import oracle as O
+
+    groups = w["groups"]
+    cx, cy = sample_cutoff
+    n = sum(len(c) for c, _, _ in groups)
+    terms = n * 2 * cx * cy
+    cores = len(os.sched_getaffinity(0))
+    if O.ref_available():
+        R = O.RefRenderer(groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
+        t0 = time.perf_counter()
+        R.fourier_transform()
+        dt = time.perf_counter() - t0
+        R.close()
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        for cons, radii, basis in groups:
+            O.slice_sum(cons, radii, basis, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0))
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return {"value": terms / dt / 1e9, "unit": "GTerms/s", "cores": cores, "kind": kind,
+            "sample": f"reference fourier_transform (direct slice sum) of all {n} particles over one z-normal "
+                      f"slice of 2*{cx}*{cy}={2 * cx * cy} frequencies ({terms:.3e} terms, {dt:.2f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle as O
+
+    w = workload(args.workload)
+    cx, cy = (32, 32)
+    groups = w["groups"]
+    n = sum(len(c) for c, _, _ in groups)
+    terms = n * 2 * cx * cy
+    cores = len(os.sched_getaffinity(0))
+    kind = "reference" if O.ref_available() else "port"
+    if kind == "reference":
+        R = O.RefRenderer(groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
+        fn = R.fourier_transform
+    else:
+        def fn():
+            for cons, radii, basis in groups:
+                O.slice_sum(cons, radii, basis, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0))
+    for _ in range(args.warmup):
+        fn()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn()
+    dt = time.perf_counter() - t0
+    value = terms * args.steps / dt / 1e9
+    sample = (f"per step: the reference's fourier_transform (OpenMP, {cores} threads) over all {n} particles of "
+              f"workload {w['name']} and one slice of {2 * cx * cy} frequencies ({terms:.3e} terms)")
+    line = {"impl": "reference", "metric": "GTerms/s (particle x frequency terms per second)", "value": value,
+            "unit": "GTerms/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["name"], "particles": n, "sample_frequencies": 2 * cx * cy},
+            "cpu_baseline": {"value": value, "unit": "GTerms/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "GTerms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if kind == "reference":
+        R.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from libmeshlessvis_b200 import meshless as M
+
+    form = {"auto": M.FORM_AUTO, "plain": M.FORM_PLAIN, "tensor": M.FORM_TENSOR}[args.form]
+    w = workload(args.workload)
+    terms, n, g = terms_per_step(w)
+    views = w["views"]
+    nv = len(views)
+    u = np.array([v[0] for v in views], np.float32)
+    v = np.array([v[1] for v in views], np.float32)
+    nx, ny = w["samples"]
+
+    lib = M.lib()
+    cfg = M.Config(step=w["step"], cutoff=w["cutoff"], samples=w["samples"], block_length=64)
+    stream = torch.cuda.Stream()
+    cfg.set_stream(stream.cuda_stream)
+    ds = M.Dataset(w["groups"])
+    cfg.register(ds)
+    sp = M.Spectrum(w["grid"], w["step3"])
+    d_images = torch.empty((nv, nx, ny), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step():
+        sp.compute(cfg, ds, form)
+        sp.render_views(cfg, u, v, d_images=d_images.data_ptr(), to_host=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    cfg.synchronize()
+    cfg.enable_timing(True)
+    for st in (M.STAGE_SUM, M.STAGE_SLICE, M.STAGE_FFT):
+        cfg.kernel_time(st)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(torch.cuda.current_device())
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.vis_kernel_launch_count()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = lib.vis_kernel_launch_count() - launches0
+    clk = clocks.stop()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    sum_ms, sum_n = cfg.kernel_time(M.STAGE_SUM)
+    sl_ms, sl_n = cfg.kernel_time(M.STAGE_SLICE)
+    fft_ms, fft_n = cfg.kernel_time(M.STAGE_FFT)
+    cfg.enable_timing(False)
+    t_max = allmax(t_ms)
+    sec = t_max / 1000.0
+    value = world * terms * args.steps / sec / 1e9
+    views_per_s = world * nv * args.steps / sec
+
+    # dominant kernel: the Fourier-sum kernel(s)
+    peaks, peak_src = measured_peaks()
+    sum_launch_ms = sum_ms / max(1, sum_n)
+    terms_per_launch = terms * args.steps / max(1, sum_n)
+    achieved_tflops = 8.0 * terms_per_launch / (sum_launch_ms / 1000.0) / 1e12
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    max_mhz = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved_tflops / fp32_peak, "traffic": None,
+                "kernel": "plain_sum_kernel", "flops_per_term": 8,
+                "peak_source": f"nominal FP32: {sm_count} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x {max_mhz:.0f} MHz "
+                               "(MEASURED_PEAKS.json has no FP32 figure)"}
+    if clk.get("sm_mhz"):
+        roofline["frac_at_sampled_clock"] = achieved_tflops / (fp32_peak * clk["sm_mhz"] / max_mhz)
+
+    # end to end through the public C API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pinned = []
+        groups = []
+        h2d = 0
+        for cons, radii, basis in w["groups"]:
+            tc = torch.empty(len(cons) * 16, dtype=torch.uint8, pin_memory=True)
+            pc = tc.numpy().view(cons.dtype)
+            pc[:] = cons
+            pinned.append(tc)
+            h2d += pc.nbytes
+            pr = None
+            if radii is not None:
+                tr = torch.empty(len(radii), dtype=torch.float32, pin_memory=True)
+                pr = tr.numpy()
+                pr[:] = radii
+                pinned.append(tr)
+                h2d += pr.nbytes
+            groups.append((pc, pr, basis))
+        ds2 = M.Dataset(groups)
+        h_images = torch.empty((nv, nx, ny), dtype=torch.float32, pin_memory=True)
+        d2h = h_images.numel() * 4
+
+        def e2e_step():
+            cfg.register(ds2)
+            sp.compute(cfg, ds2, form)
+            lib.vis_spectrum_render_views(sp.ptr, cfg.ptr, nv, u.ctypes.data, v.ctypes.data, None,
+                                          h_images.data_ptr())
+            cfg.unregister(ds2)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                e_ev[k][0].record(stream)
+                e2e_step()
+                e_ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e_ms = allmax(sum(a.elapsed_time(b) for a, b in e_ev))
+        e2e = {"value": world * terms * args.steps / (e_ms / 1000.0) / 1e9, "unit": "GTerms/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms / args.steps,
+               "wall_ms_per_step": wall * 1000 / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w)
+
+    sp.close()
+    cfg.unregister(ds)
+    cfg.close()
+    if rank == 0:
+        line = {"metric": "GTerms/s (particle x frequency terms per second; 3D half-spectrum sum + all views)",
+                "value": value, "unit": "GTerms/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE config shapes)",
+                "config": {"workload": w["name"], "particles": n, "grid": list(w["grid"]),
+                           "half_spectrum": g, "views": nv, "image": [nx, ny], "form": args.form,
+                           "l2": "flushed between timed steps (256 MB write outside the event pair)",
+                           "parallelism": f"replicas x{world}"},
+                "views_per_s": views_per_s,
+                "stages_ms_per_step": {"sum": sum_ms / args.steps, "slice": sl_ms / args.steps,
+                                       "fft": fft_ms / args.steps},
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
+                "peaks_source": peak_src}
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

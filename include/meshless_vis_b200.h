@@ -1,0 +1,121 @@
+/*
+ * meshless_vis_b200.h -- additions of the B200 drop-in that have no
+ * counterpart in the reference's C API.  Everything here is extern "C", with
+ * plain pointers and sizes.
+ *
+ *   - error reporting (the reference aborts through cutil macros instead,
+ *     meshless_vis/meshless_vis.cu:73-81, :141-146);
+ *   - an explicit CUDA stream per VisConfig (the reference uses the default
+ *     stream everywhere, meshless_vis/meshless_vis.cu:334-350);
+ *   - the 3D Hermitian half-spectrum path: the Fourier sum is evaluated once on
+ *     a 3D lattice, and any number of views are then cut from it by
+ *     interpolated Fourier slices and rendered by one batched 2D C2R, instead
+ *     of redoing the whole sum per view as vis_fourier_volume_rendering does;
+ *   - per-stage device timing for benchmarks.
+ */
+#ifndef MESHLESS_VIS_B200_H
+#define MESHLESS_VIS_B200_H
+
+#include "meshless_vis.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- errors */
+enum VisError
+{
+    VIS_SUCCESS = 0,
+    VIS_ERROR_INVALID_VALUE = 1, /* bad argument, NULL pointer, size out of range */
+    VIS_ERROR_INVALID_CONFIG = 2, /* vis_config_check() would return false */
+    VIS_ERROR_CUDA = 3,           /* a CUDA runtime call failed */
+    VIS_ERROR_CUFFT = 4,          /* a cuFFT call failed */
+    VIS_ERROR_OUT_OF_MEMORY = 5,  /* device allocation failed */
+    VIS_ERROR_NOT_REGISTERED = 6, /* dataset not registered with vis_register_meshless_dataset */
+    VIS_ERROR_UNSUPPORTED = 7,    /* feature not available (OpenGL interop) */
+    VIS_ERROR_NO_KERNEL = 8       /* the library was built without code for this device */
+};
+
+/* Code of the last failed call on this host thread (VIS_SUCCESS if none since
+ * the last vis_clear_last_error). */
+int vis_get_last_error(void);
+/* Human-readable detail of the last failure on this host thread. */
+const char* vis_get_last_error_message(void);
+const char* vis_get_error_string(int code);
+void vis_clear_last_error(void);
+
+/* ---------------------------------------------------------------- streams */
+/* All work for a VisConfig is issued on its stream (default: a non-blocking
+ * stream the library creates).  vis_copy_to_host synchronises it. */
+int vis_config_set_stream(VisConfig* vis_config, cudaStream_t stream);
+cudaStream_t vis_config_get_stream(VisConfig* vis_config);
+int vis_config_synchronize(VisConfig* vis_config);
+
+/* ------------------------------------------------------- 3D half-spectrum */
+/* How the Fourier sum is evaluated:
+ *   VIS_FORM_PLAIN  -- FP32 SIMT, exact fixed-point phase per term;
+ *   VIS_FORM_TENSOR -- per-axis exponential factorisation as complex GEMMs on
+ *                      the tensor cores (split FP16 hi+lo, FP32 accumulate);
+ *                      needs a separable basis (GAUSSIAN_DECAYING, GAUSSIAN) or
+ *                      a group without radii; other groups fall back to PLAIN;
+ *   VIS_FORM_AUTO   -- TENSOR where the group allows it, else PLAIN. */
+enum VisSumForm
+{
+    VIS_FORM_AUTO = 0,
+    VIS_FORM_PLAIN = 1,
+    VIS_FORM_TENSOR = 2
+};
+
+typedef struct VisSpectrum VisSpectrum;
+
+/* A device-resident half-spectrum F(k) = sum_j w_j Phi^(|k| h_j)
+ * exp(-2 pi i k.x_j) on k = step_size * (i, j, l), i in [-Kx/2, Kx/2),
+ * j in [-Ky/2, Ky/2), l in [0, Kz/2]; grid_size = (Kx, Ky, Kz), each even and
+ * >= 2.  Storage: float2[Kx][Ky][Kz/2+1], element [i+Kx/2][j+Ky/2][l]. */
+VisSpectrum* vis_spectrum_create(int3 grid_size, float step_size);
+void vis_spectrum_destroy(VisSpectrum* spectrum);
+int3 vis_spectrum_grid_size(VisSpectrum* spectrum);
+float2* vis_spectrum_device_data(VisSpectrum* spectrum);
+
+/* Evaluates the spectrum of every group of a registered dataset (the first
+ * group overwrites, later groups accumulate), on vis_config's stream. */
+int vis_spectrum_compute(VisSpectrum* spectrum, VisConfig* vis_config, MeshlessDataset* meshless_dataset, int form);
+
+/* Copies the whole spectrum to the host (Kx*Ky*(Kz/2+1) float2) and waits. */
+int vis_spectrum_copy_to_host(VisSpectrum* spectrum, VisConfig* vis_config, float2* h_spectrum);
+
+/* Renders number_of_views views from the spectrum with vis_config's step_size,
+ * cutoff and number of samples: per view, slice sample (x, y) with
+ * x in (-cx, cx), y in [0, cy) takes the trilinearly interpolated spectrum at
+ * step.x x u + step.y y v (Hermitian fold for k_z < 0, zero outside the
+ * lattice), times step.x*step.y, placed in the C2R layout of arrange_samples
+ * (meshless_vis/meshless_vis.cu:318-332); then one batched unnormalised 2D C2R.
+ * u_axes, v_axes: host arrays of number_of_views float3.
+ * d_images: device float[views][Nx][Ny], or NULL to use a library buffer;
+ * h_images: if not NULL, the images are also copied there and the call waits. */
+int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int number_of_views,
+                              const float3* u_axes, const float3* v_axes, float* d_images, float* h_images);
+
+/* ----------------------------------------------------------------- timing */
+enum VisTimingStage
+{
+    VIS_STAGE_SUM = 0,   /* Fourier-sum kernels (direct slice and 3D spectrum) */
+    VIS_STAGE_SLICE = 1, /* slice extraction into the C2R layout */
+    VIS_STAGE_FFT = 2    /* cuFFT C2R */
+};
+/* When enabled, CUDA events bracket every launch of each stage on the
+ * config's stream.  vis_config_kernel_timing waits for them, returns the summed
+ * device time (ms) and launch count of a stage since the last query, and
+ * resets that stage. */
+int vis_config_enable_kernel_timing(VisConfig* vis_config, int enable);
+int vis_config_kernel_timing(VisConfig* vis_config, int stage, float* total_ms, int* launches);
+
+/* Number of this library's own CUDA kernels launched by the process so far
+ * (cuFFT's kernels are not counted). */
+unsigned long long vis_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

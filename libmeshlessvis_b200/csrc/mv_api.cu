@@ -1,0 +1,782 @@
+// C API of the drop-in: include/meshless_vis.h (the reference's
+// meshless_vis/meshless_vis.cu:129-364 interface) and the additions of
+// include/meshless_vis_b200.h.
+//
+// Host-side design:
+//   - VisConfig keeps the reference's public layout; everything new (stream,
+//     split-K workspace, batched cuFFT plans, timing events) lives in a side
+//     table keyed by the VisConfig pointer.
+//   - Every call validates its arguments, never exits, records failures in a
+//     thread-local error (vis_get_last_error) and returns early.
+//   - All device work of a config is stream-ordered on its stream; only
+//     vis_copy_to_host, vis_spectrum_copy_to_host, registration and the
+//     host-image variant of vis_spectrum_render_views wait for it.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include <cufft.h>
+
+#include "meshless_vis_b200.h"
+#include "mv_internal.h"
+
+namespace mv {
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local int t_last_error = kOk;
+thread_local std::string t_last_message;
+}  // namespace
+
+int set_error(int code, const std::string& message) {
+    t_last_error = code;
+    t_last_message = message;
+    return code;
+}
+
+int check_cuda(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return kOk;
+    const int code = (err == cudaErrorMemoryAllocation) ? kOutOfMemory
+                     : (err == cudaErrorNoKernelImageForDevice || err == cudaErrorInvalidDeviceFunction) ? kNoKernel
+                                                                                                        : kCudaError;
+    return set_error(code, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+static int check_cufft(cufftResult r, const char* what) {
+    if (r == CUFFT_SUCCESS) return kOk;
+    return set_error(r == CUFFT_ALLOC_FAILED ? kOutOfMemory : kCufftError,
+                     std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+
+int device_sm_count() {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    cache[dev] = sms;
+    return sms;
+}
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// --------------------------------------------------------------- workspace
+int Workspace::reserve(size_t need) {
+    if (need <= bytes) return kOk;
+    if (ptr) {
+        // The buffer may still be read by earlier launches on any stream.
+        cudaDeviceSynchronize();
+        cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    const size_t grow = std::max(need, (size_t)1 << 20);
+    cudaError_t e = cudaMalloc(&ptr, grow);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        cudaGetLastError();
+        return check_cuda(e, "workspace cudaMalloc");
+    }
+    bytes = grow;
+    return kOk;
+}
+
+void Workspace::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// ------------------------------------------------------------------ timing
+struct KernelTimer {
+    bool enabled = false;
+    cudaEvent_t open[3] = {nullptr, nullptr, nullptr};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> done[3];
+    std::vector<cudaEvent_t> pool;
+
+    cudaEvent_t take() {
+        cudaEvent_t e = nullptr;
+        if (!pool.empty()) {
+            e = pool.back();
+            pool.pop_back();
+        } else if (cudaEventCreate(&e) != cudaSuccess) {
+            e = nullptr;
+        }
+        return e;
+    }
+    void clear_stage(int s) {
+        for (auto& p : done[s]) {
+            pool.push_back(p.first);
+            pool.push_back(p.second);
+        }
+        done[s].clear();
+    }
+    ~KernelTimer() {
+        for (int s = 0; s < 3; ++s) {
+            clear_stage(s);
+            if (open[s]) pool.push_back(open[s]);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+void timer_begin(KernelTimer* t, int stage, cudaStream_t stream) {
+    if (!t || !t->enabled) return;
+    cudaEvent_t e = t->take();
+    if (!e) return;
+    cudaEventRecord(e, stream);
+    if (t->open[stage]) t->pool.push_back(t->open[stage]);
+    t->open[stage] = e;
+}
+
+void timer_end(KernelTimer* t, int stage, cudaStream_t stream) {
+    if (!t || !t->enabled || !t->open[stage]) return;
+    cudaEvent_t e = t->take();
+    if (!e) return;
+    cudaEventRecord(e, stream);
+    t->done[stage].emplace_back(t->open[stage], e);
+    t->open[stage] = nullptr;
+}
+
+// ------------------------------------------------------------- config state
+struct ConfigState {
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Workspace partials;  // split-K partial sums
+    Workspace arranged;  // batched C2R inputs of vis_spectrum_render_views
+    Workspace images;    // library-owned batched images
+    Workspace views;     // per-view parameters
+    std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
+    KernelTimer timer;
+
+    ~ConfigState() {
+        if (stream) cudaStreamSynchronize(stream);
+        partials.release();
+        arranged.release();
+        images.release();
+        views.release();
+        for (auto& kv : batched_plans) cufftDestroy(kv.second);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+std::mutex g_mu;
+std::unordered_map<const VisConfig*, ConfigState*> g_states;
+
+ConfigState* state_of(const VisConfig* cfg) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_states.find(cfg);
+    return it == g_states.end() ? nullptr : it->second;
+}
+
+bool valid_config(const VisConfig* c, std::string* why) {
+    // meshless_vis/meshless_vis.cu:191-210
+    auto fail = [&](const char* m) {
+        if (why) *why = m;
+        return false;
+    };
+    if (c->block_length < 64) return fail("block_length < 64");
+    if (c->block_length < 32) return fail("block_length < warp size");
+    if (c->block_length > 1024) return fail("block_length > max threads per block");
+    if (c->_cutoff_frequency.x < 0 || c->_cutoff_frequency.y < 0) return fail("negative cutoff frequency");
+    if ((2LL * c->_cutoff_frequency.x * c->_cutoff_frequency.y) % c->block_length) return fail("2*cx*cy is not a multiple of block_length");
+    if (2 * c->_cutoff_frequency.x > c->_number_of_samples.x) return fail("2*cutoff.x > number_of_samples.x");
+    if (2 * c->_cutoff_frequency.y > c->_number_of_samples.y) return fail("2*cutoff.y > number_of_samples.y");
+    if (c->_number_of_partial_sums < 1) return fail("number_of_partial_sums < 1");
+    return true;
+}
+
+template <typename T>
+int device_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return kOk;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return check_cuda(e, "cudaMalloc");
+    }
+    return kOk;
+}
+
+size_t freq_image_count(const VisConfig* c) {
+    return 2ULL * std::max(0, c->_cutoff_frequency.x) * std::max(0, c->_cutoff_frequency.y) *
+           std::max(1, c->_number_of_partial_sums);
+}
+size_t arranged_count(const VisConfig* c) {
+    return (size_t)std::max(0, c->_number_of_samples.x) * (std::max(0, c->_number_of_samples.y) / 2 + 1);
+}
+size_t image_count(const VisConfig* c) {
+    return (size_t)std::max(0, c->_number_of_samples.x) * std::max(0, c->_number_of_samples.y);
+}
+
+int make_plan(VisConfig* c) {
+    c->_plan = 0;
+    if (c->_number_of_samples.x < 1 || c->_number_of_samples.y < 2) return kOk;
+    return check_cufft(cufftPlan2d(&c->_plan, c->_number_of_samples.x, c->_number_of_samples.y, CUFFT_C2R),
+                       "cufftPlan2d");
+}
+
+}  // namespace
+
+}  // namespace mv
+
+using namespace mv;
+
+// ====================================================================== C ABI
+extern "C" {
+
+int vis_get_last_error(void) { return t_last_error; }
+const char* vis_get_last_error_message(void) { return t_last_message.c_str(); }
+void vis_clear_last_error(void) {
+    t_last_error = kOk;
+    t_last_message.clear();
+}
+const char* vis_get_error_string(int code) {
+    switch (code) {
+    case VIS_SUCCESS: return "success";
+    case VIS_ERROR_INVALID_VALUE: return "invalid value";
+    case VIS_ERROR_INVALID_CONFIG: return "invalid configuration";
+    case VIS_ERROR_CUDA: return "CUDA error";
+    case VIS_ERROR_CUFFT: return "cuFFT error";
+    case VIS_ERROR_OUT_OF_MEMORY: return "out of device memory";
+    case VIS_ERROR_NOT_REGISTERED: return "dataset not registered";
+    case VIS_ERROR_UNSUPPORTED: return "unsupported";
+    case VIS_ERROR_NO_KERNEL: return "no kernel image for this device";
+    default: return "unknown error";
+    }
+}
+
+// meshless_vis/meshless_vis.cu:129-176 (device-property printout dropped).
+VisConfig* vis_config_create(bool automatic_d_image, float2 step_size, int2 cutoff_frequency, float3 u_axis,
+                             float3 v_axis, int2 number_of_samples, int block_length, int number_of_partial_sums) {
+    if (cutoff_frequency.x < 0 || cutoff_frequency.y < 0 || number_of_samples.x < 1 || number_of_samples.y < 2) {
+        set_error(kInvalidValue, "vis_config_create: cutoff must be >= 0 and number_of_samples >= (1, 2)");
+        return nullptr;
+    }
+    VisConfig* c = (VisConfig*)std::calloc(1, sizeof(VisConfig));
+    if (!c) {
+        set_error(kOutOfMemory, "vis_config_create: host allocation failed");
+        return nullptr;
+    }
+    c->step_size = step_size;
+    c->u_axis = u_axis;
+    c->v_axis = v_axis;
+    c->cull_fully_aliased_terms = false;
+    c->_number_of_samples = number_of_samples;
+    c->_cutoff_frequency = cutoff_frequency;
+    c->block_length = block_length;
+    c->_number_of_partial_sums = number_of_partial_sums;
+    c->_automatic_d_image = automatic_d_image;
+    c->_scale = step_size.x * step_size.y;
+
+    ConfigState* s = new ConfigState();
+    int st = check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    s->own_stream = st == kOk;
+    if (st == kOk) st = device_alloc(&c->_d_freq_image, freq_image_count(c));
+    if (st == kOk) st = device_alloc(&c->_d_freq_image_arranged, arranged_count(c));
+    if (st == kOk && automatic_d_image) st = device_alloc(&c->_d_image, image_count(c));
+    if (st == kOk) st = make_plan(c);
+    if (st != kOk) {
+        cudaFree(c->_d_freq_image);
+        cudaFree(c->_d_freq_image_arranged);
+        if (automatic_d_image) cudaFree(c->_d_image);
+        if (c->_plan) cufftDestroy(c->_plan);
+        delete s;
+        std::free(c);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_states[c] = s;
+    return c;
+}
+
+// meshless_vis/meshless_vis.cu:178-189 (the CUDA build's defaults).
+VisConfig* vis_config_get_default(void) {
+    return vis_config_create(true, make_float2(0.1f, 0.1f), make_int2(128, 128), make_float3(1.f, 0.f, 0.f),
+                             make_float3(0.f, 1.f, 0.f), make_int2(512, 512), 256, 1);
+}
+
+bool vis_config_check(VisConfig* vis_config) {
+    if (!vis_config) {
+        set_error(kInvalidValue, "vis_config_check: NULL config");
+        return false;
+    }
+    return valid_config(vis_config, nullptr);
+}
+
+// The reference overwrites _d_image (meshless_vis/meshless_vis.cu:244-247) and
+// would later cudaFree the caller's buffer in vis_config_destroy; here an owned
+// image is released first and the caller keeps ownership of theirs.
+void vis_config_manual_d_image(VisConfig* vis_config, void* d_image) {
+    if (!vis_config) {
+        set_error(kInvalidValue, "vis_config_manual_d_image: NULL config");
+        return;
+    }
+    if (vis_config->_automatic_d_image && vis_config->_d_image) {
+        ConfigState* s = state_of(vis_config);
+        if (s) cudaStreamSynchronize(s->stream);
+        cudaFree(vis_config->_d_image);
+    }
+    vis_config->_automatic_d_image = false;
+    vis_config->_d_image = static_cast<float*>(d_image);
+}
+
+// meshless_vis/meshless_vis.cu:212-227
+void vis_config_change_number_of_samples(VisConfig* c, int2 number_of_samples) {
+    if (!c || number_of_samples.x < 1 || number_of_samples.y < 2) {
+        set_error(kInvalidValue, "vis_config_change_number_of_samples: bad arguments");
+        return;
+    }
+    ConfigState* s = state_of(c);
+    if (s) cudaStreamSynchronize(s->stream);
+    c->_number_of_samples = number_of_samples;
+    if (c->_automatic_d_image) {
+        cudaFree(c->_d_image);
+        if (device_alloc(&c->_d_image, image_count(c)) != kOk) return;
+    }
+    cudaFree(c->_d_freq_image_arranged);
+    if (device_alloc(&c->_d_freq_image_arranged, arranged_count(c)) != kOk) return;
+    if (c->_plan) cufftDestroy(c->_plan);
+    make_plan(c);
+}
+
+// meshless_vis/meshless_vis.cu:229-234
+void vis_config_change_cutoff_frequency(VisConfig* c, int2 cutoff_frequency) {
+    if (!c || cutoff_frequency.x < 0 || cutoff_frequency.y < 0) {
+        set_error(kInvalidValue, "vis_config_change_cutoff_frequency: bad arguments");
+        return;
+    }
+    ConfigState* s = state_of(c);
+    if (s) cudaStreamSynchronize(s->stream);
+    c->_cutoff_frequency = cutoff_frequency;
+    cudaFree(c->_d_freq_image);
+    device_alloc(&c->_d_freq_image, freq_image_count(c));
+}
+
+// meshless_vis/meshless_vis.cu:236-242
+void vis_config_change_number_of_partial_sums(VisConfig* c, int number_of_partial_sums) {
+    if (!c) {
+        set_error(kInvalidValue, "vis_config_change_number_of_partial_sums: NULL config");
+        return;
+    }
+    ConfigState* s = state_of(c);
+    if (s) cudaStreamSynchronize(s->stream);
+    c->_number_of_partial_sums = number_of_partial_sums;
+    cudaFree(c->_d_freq_image);
+    device_alloc(&c->_d_freq_image, freq_image_count(c));
+}
+
+// meshless_vis/meshless_vis.cu:249-256
+void vis_config_destroy(VisConfig* c) {
+    if (!c) return;
+    ConfigState* s = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        auto it = g_states.find(c);
+        if (it != g_states.end()) {
+            s = it->second;
+            g_states.erase(it);
+        }
+    }
+    delete s;  // waits for the stream
+    if (c->_automatic_d_image) cudaFree(c->_d_image);
+    cudaFree(c->_d_freq_image_arranged);
+    cudaFree(c->_d_freq_image);
+    if (c->_plan) cufftDestroy(c->_plan);
+    std::free(c);
+}
+
+// meshless_vis/meshless_vis.cu:258-262
+void vis_config_compute_scale(VisConfig* c) {
+    if (!c) {
+        set_error(kInvalidValue, "vis_config_compute_scale: NULL config");
+        return;
+    }
+    c->_scale = c->step_size.x * c->step_size.y;
+}
+
+int vis_config_set_stream(VisConfig* c, cudaStream_t stream) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s) return set_error(kInvalidValue, "vis_config_set_stream: unknown config");
+    cudaStreamSynchronize(s->stream);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->own_stream = false;
+    s->stream = stream;
+    return kOk;
+}
+
+cudaStream_t vis_config_get_stream(VisConfig* c) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s) {
+        set_error(kInvalidValue, "vis_config_get_stream: unknown config");
+        return nullptr;
+    }
+    return s->stream;
+}
+
+int vis_config_synchronize(VisConfig* c) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s) return set_error(kInvalidValue, "vis_config_synchronize: unknown config");
+    return check_cuda(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+}
+
+// meshless_vis/meshless_vis.cu:264-290: device copies padded with zeros to a
+// multiple of number_of_partial_sums * block_length (d_number_of_terms).
+void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s || !ds || (ds->number_of_groups > 0 && !ds->groups)) {
+        set_error(kInvalidValue, "vis_register_meshless_dataset: NULL or unknown argument");
+        return;
+    }
+    const long long multiple = std::max(1LL, (long long)std::max(1, c->_number_of_partial_sums) * std::max(1, c->block_length));
+    for (int g = 0; g < ds->number_of_groups; ++g) {
+        Group& grp = ds->groups[g];
+        grp.d_constraints = nullptr;
+        grp.d_radii = nullptr;
+        grp.d_number_of_terms = 0;
+        if (grp.number_of_terms < 0 || (grp.number_of_terms > 0 && !grp.h_constraints)) {
+            set_error(kInvalidValue, "vis_register_meshless_dataset: group without host constraints");
+            return;
+        }
+        const long long padded = (grp.number_of_terms + multiple - 1) / multiple * multiple;
+        if (padded > INT32_MAX) {
+            set_error(kInvalidValue, "vis_register_meshless_dataset: too many terms");
+            return;
+        }
+        grp.d_number_of_terms = (int)padded;
+        if (padded == 0) continue;
+        if (device_alloc(&grp.d_constraints, (size_t)padded) != kOk) return;
+        cudaMemsetAsync(grp.d_constraints, 0, sizeof(Constraint) * padded, s->stream);
+        cudaMemcpyAsync(grp.d_constraints, grp.h_constraints, sizeof(Constraint) * grp.number_of_terms,
+                        cudaMemcpyHostToDevice, s->stream);
+        if (grp.h_radii) {
+            if (device_alloc(&grp.d_radii, (size_t)padded) != kOk) return;
+            cudaMemsetAsync(grp.d_radii, 0, sizeof(float) * padded, s->stream);
+            cudaMemcpyAsync(grp.d_radii, grp.h_radii, sizeof(float) * grp.number_of_terms, cudaMemcpyHostToDevice,
+                            s->stream);
+        }
+    }
+    check_cuda(cudaStreamSynchronize(s->stream), "vis_register_meshless_dataset");
+}
+
+// meshless_vis/meshless_vis.cu:292-299
+void vis_unregister_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s || !ds) {
+        set_error(kInvalidValue, "vis_unregister_meshless_dataset: NULL or unknown argument");
+        return;
+    }
+    cudaStreamSynchronize(s->stream);
+    for (int g = 0; g < ds->number_of_groups; ++g) {
+        cudaFree(ds->groups[g].d_constraints);
+        cudaFree(ds->groups[g].d_radii);
+        ds->groups[g].d_constraints = nullptr;
+        ds->groups[g].d_radii = nullptr;
+    }
+}
+
+void vis_opengl_fourier_volume_rendering(MeshlessDataset*, VisConfig*, GLuint) {
+    set_error(kUnsupported, "vis_opengl_fourier_volume_rendering: no OpenGL on this build; use vis_config_manual_d_image");
+}
+
+// meshless_vis/meshless_vis.cu:334-350: direct slice sum of every group
+// (fused with reduce_partial_sums and arrange_samples), then the 2D C2R.
+void vis_fourier_volume_rendering(MeshlessDataset* ds, VisConfig* c) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s || !ds || (ds->number_of_groups > 0 && !ds->groups)) {
+        set_error(kInvalidValue, "vis_fourier_volume_rendering: NULL or unknown argument");
+        return;
+    }
+    std::string why;
+    if (!valid_config(c, &why)) {
+        set_error(kInvalidConfig, "vis_fourier_volume_rendering: " + why);
+        return;
+    }
+    if (!c->_d_image || !c->_d_freq_image_arranged) {
+        set_error(kInvalidValue, "vis_fourier_volume_rendering: no device image");
+        return;
+    }
+    vis_config_compute_scale(c);
+    const int cx = c->_cutoff_frequency.x, cy = c->_cutoff_frequency.y;
+    const int nx = c->_number_of_samples.x, ny = c->_number_of_samples.y;
+    if (check_cuda(cudaMemsetAsync(c->_d_freq_image_arranged, 0, sizeof(float2) * arranged_count(c), s->stream),
+                   "cudaMemsetAsync") != kOk)
+        return;
+    for (int g = 0; g < ds->number_of_groups; ++g) {
+        const Group& grp = ds->groups[g];
+        if (grp.number_of_terms > 0 && !grp.d_constraints) {
+            set_error(kNotRegistered, "vis_fourier_volume_rendering: group not registered");
+            return;
+        }
+        SumRequest r{};
+        r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
+        r.radii = grp.d_radii;
+        r.n = grp.number_of_terms;
+        r.basis = (int)grp.basis_function_id;
+        // Slice x in (-cx, cx): the reference also evaluates x == cx
+        // (fourier_transform.cu:248-249) and then drops it (meshless_vis.cu:323).
+        r.lat.x0 = -cx + 1;
+        r.lat.nx = cx > 0 ? 2 * cx - 1 : 0;
+        r.lat.y0 = 0;
+        r.lat.ny = cy;
+        r.lat.z0 = 0;
+        r.lat.nz = 1;
+        r.lat.kx = c->step_size.x;
+        r.lat.ky = c->step_size.y;
+        r.lat.kz = 0.0;
+        const double sx = c->step_size.x, sy = c->step_size.y;
+        const double m[9] = {sx * c->u_axis.x, sx * c->u_axis.y, sx * c->u_axis.z,
+                             sy * c->v_axis.x, sy * c->v_axis.y, sy * c->v_axis.z, 0.0, 0.0, 0.0};
+        std::memcpy(r.lat.m, m, sizeof(m));
+        r.scale = (double)c->step_size.x * (double)c->step_size.y;
+        r.out = c->_d_freq_image_arranged;
+        r.wrap = nx;
+        r.row = ny / 2 + 1;
+        r.accumulate = g > 0;
+        r.stream = s->stream;
+        if (launch_plain_sum(r, s->partials, &s->timer) != kOk) return;
+    }
+    if (check_cufft(cufftSetStream(c->_plan, s->stream), "cufftSetStream") != kOk) return;
+    timer_begin(&s->timer, 2, s->stream);
+    cufftResult fr = cufftExecC2R(c->_plan, reinterpret_cast<cufftComplex*>(c->_d_freq_image_arranged), c->_d_image);
+    timer_end(&s->timer, 2, s->stream);
+    check_cufft(fr, "cufftExecC2R");
+}
+
+// meshless_vis/meshless_vis.cu:352-355
+void vis_copy_to_host(VisConfig* c, float* h_image) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s || !h_image || !c->_d_image) {
+        set_error(kInvalidValue, "vis_copy_to_host: NULL or unknown argument");
+        return;
+    }
+    if (check_cuda(cudaMemcpyAsync(h_image, c->_d_image, sizeof(float) * image_count(c), cudaMemcpyDeviceToHost,
+                                   s->stream),
+                   "vis_copy_to_host") != kOk)
+        return;
+    check_cuda(cudaStreamSynchronize(s->stream), "vis_copy_to_host");
+}
+
+// ------------------------------------------------------------------ timing
+unsigned long long vis_kernel_launch_count(void) { return g_launches.load(); }
+
+int vis_config_enable_kernel_timing(VisConfig* c, int enable) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s) return set_error(kInvalidValue, "vis_config_enable_kernel_timing: unknown config");
+    s->timer.enabled = enable != 0;
+    return kOk;
+}
+
+int vis_config_kernel_timing(VisConfig* c, int stage, float* total_ms, int* launches) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s || stage < 0 || stage > 2) return set_error(kInvalidValue, "vis_config_kernel_timing: bad arguments");
+    float total = 0.f;
+    int count = 0;
+    for (auto& p : s->timer.done[stage]) {
+        if (cudaEventSynchronize(p.second) != cudaSuccess) continue;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
+            total += ms;
+            ++count;
+        }
+    }
+    s->timer.clear_stage(stage);
+    if (total_ms) *total_ms = total;
+    if (launches) *launches = count;
+    return kOk;
+}
+
+}  // extern "C"
+
+// ================================================================ spectrum
+struct VisSpectrum {
+    int3 grid;
+    float step;
+    float2* data;
+    size_t count;
+};
+
+namespace mv {
+int tensor_sum_available(const SumRequest& req);  // mv_tc_sum.cu
+int launch_tensor_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer);
+}  // namespace mv
+
+extern "C" {
+
+VisSpectrum* vis_spectrum_create(int3 grid_size, float step_size) {
+    const int3 g = grid_size;
+    if (g.x < 2 || g.y < 2 || g.z < 2 || (g.x & 1) || (g.y & 1) || (g.z & 1) || !(step_size > 0.f)) {
+        set_error(kInvalidValue, "vis_spectrum_create: grid extents must be even and >= 2, step > 0");
+        return nullptr;
+    }
+    const size_t count = (size_t)g.x * g.y * (g.z / 2 + 1);
+    if ((double)g.x * g.y * (g.z / 2 + 1) > (double)INT32_MAX) {
+        set_error(kInvalidValue, "vis_spectrum_create: grid too large");
+        return nullptr;
+    }
+    VisSpectrum* sp = new VisSpectrum{g, step_size, nullptr, count};
+    if (device_alloc(&sp->data, count) != kOk) {
+        delete sp;
+        return nullptr;
+    }
+    return sp;
+}
+
+void vis_spectrum_destroy(VisSpectrum* sp) {
+    if (!sp) return;
+    cudaDeviceSynchronize();
+    cudaFree(sp->data);
+    delete sp;
+}
+
+int3 vis_spectrum_grid_size(VisSpectrum* sp) { return sp ? sp->grid : make_int3(0, 0, 0); }
+float2* vis_spectrum_device_data(VisSpectrum* sp) { return sp ? sp->data : nullptr; }
+
+int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int form) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!sp || !s || !ds || (ds->number_of_groups > 0 && !ds->groups))
+        return set_error(kInvalidValue, "vis_spectrum_compute: NULL or unknown argument");
+    if (form < VIS_FORM_AUTO || form > VIS_FORM_TENSOR) return set_error(kInvalidValue, "vis_spectrum_compute: bad form");
+    if (ds->number_of_groups == 0)
+        return check_cuda(cudaMemsetAsync(sp->data, 0, sizeof(float2) * sp->count, s->stream), "cudaMemsetAsync");
+    for (int g = 0; g < ds->number_of_groups; ++g) {
+        const Group& grp = ds->groups[g];
+        if (grp.number_of_terms > 0 && !grp.d_constraints)
+            return set_error(kNotRegistered, "vis_spectrum_compute: group not registered");
+        SumRequest r{};
+        r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
+        r.radii = grp.d_radii;
+        r.n = grp.number_of_terms;
+        r.basis = (int)grp.basis_function_id;
+        r.lat.x0 = -sp->grid.x / 2;
+        r.lat.nx = sp->grid.x;
+        r.lat.y0 = -sp->grid.y / 2;
+        r.lat.ny = sp->grid.y;
+        r.lat.z0 = 0;
+        r.lat.nz = sp->grid.z / 2 + 1;
+        r.lat.kx = r.lat.ky = r.lat.kz = sp->step;
+        const double st = sp->step;
+        const double m[9] = {st, 0, 0, 0, st, 0, 0, 0, st};
+        std::memcpy(r.lat.m, m, sizeof(m));
+        r.scale = 1.0;
+        r.out = sp->data;
+        r.wrap = 0;
+        r.row = 0;
+        r.accumulate = g > 0;
+        r.stream = s->stream;
+        int rc;
+        const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
+        if (want_tc && tensor_sum_available(r)) rc = launch_tensor_sum(r, s->partials, &s->timer);
+        else rc = launch_plain_sum(r, s->partials, &s->timer);
+        if (rc != kOk) return rc;
+    }
+    return kOk;
+}
+
+int vis_spectrum_copy_to_host(VisSpectrum* sp, VisConfig* c, float2* h) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!sp || !s || !h) return set_error(kInvalidValue, "vis_spectrum_copy_to_host: NULL or unknown argument");
+    int rc = check_cuda(cudaMemcpyAsync(h, sp->data, sizeof(float2) * sp->count, cudaMemcpyDeviceToHost, s->stream),
+                        "vis_spectrum_copy_to_host");
+    if (rc != kOk) return rc;
+    return check_cuda(cudaStreamSynchronize(s->stream), "vis_spectrum_copy_to_host");
+}
+
+int vis_spectrum_render_views(VisSpectrum* sp, VisConfig* c, int number_of_views, const float3* u_axes,
+                              const float3* v_axes, float* d_images, float* h_images) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!sp || !s || number_of_views < 0 || (number_of_views > 0 && (!u_axes || !v_axes)))
+        return set_error(kInvalidValue, "vis_spectrum_render_views: NULL or unknown argument");
+    if (number_of_views == 0) return kOk;
+    const int cx = c->_cutoff_frequency.x, cy = c->_cutoff_frequency.y;
+    const int nx = c->_number_of_samples.x, ny = c->_number_of_samples.y;
+    if (cx < 0 || cy < 0 || 2 * cx > nx || 2 * cy > ny || nx < 1 || ny < 2)
+        return set_error(kInvalidConfig, "vis_spectrum_render_views: cutoff/number_of_samples mismatch");
+
+    std::vector<float> hv((size_t)8 * number_of_views);
+    for (int i = 0; i < number_of_views; ++i) {
+        float* p = hv.data() + 8 * i;
+        p[0] = u_axes[i].x; p[1] = u_axes[i].y; p[2] = u_axes[i].z;
+        p[3] = v_axes[i].x; p[4] = v_axes[i].y; p[5] = v_axes[i].z;
+        p[6] = c->step_size.x; p[7] = c->step_size.y;
+    }
+    const size_t per_arr = (size_t)nx * (ny / 2 + 1), per_img = (size_t)nx * ny;
+    int rc = s->views.reserve(hv.size() * sizeof(float));
+    if (rc == kOk) rc = s->arranged.reserve(per_arr * number_of_views * sizeof(float2));
+    if (rc == kOk && !d_images) rc = s->images.reserve(per_img * number_of_views * sizeof(float));
+    if (rc != kOk) return rc;
+    float* imgs = d_images ? d_images : static_cast<float*>(s->images.ptr);
+    rc = check_cuda(cudaMemcpyAsync(s->views.ptr, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, s->stream),
+                    "view parameters H2D");
+    if (rc != kOk) return rc;
+
+    SliceRequest q{};
+    q.spectrum = sp->data;
+    q.gx = sp->grid.x;
+    q.gy = sp->grid.y;
+    q.gz = sp->grid.z;
+    q.inv_step = 1.0f / sp->step;
+    q.views = static_cast<const float*>(s->views.ptr);
+    q.number_of_views = number_of_views;
+    q.cx = cx;
+    q.cy = cy;
+    q.nx = nx;
+    q.ny = ny;
+    q.arranged = static_cast<float2*>(s->arranged.ptr);
+    q.stream = s->stream;
+    rc = launch_slice_extract(q, &s->timer);
+    if (rc != kOk) return rc;
+
+    auto key = std::make_tuple(nx, ny, number_of_views);
+    cufftHandle plan;
+    auto it = s->batched_plans.find(key);
+    if (it == s->batched_plans.end()) {
+        if (s->batched_plans.size() >= 4) {
+            cudaStreamSynchronize(s->stream);
+            for (auto& kv : s->batched_plans) cufftDestroy(kv.second);
+            s->batched_plans.clear();
+        }
+        int n[2] = {nx, ny};
+        rc = check_cufft(cufftPlanMany(&plan, 2, n, nullptr, 1, (int)per_arr, nullptr, 1, (int)per_img, CUFFT_C2R,
+                                       number_of_views),
+                         "cufftPlanMany");
+        if (rc != kOk) return rc;
+        s->batched_plans[key] = plan;
+    } else {
+        plan = it->second;
+    }
+    rc = check_cufft(cufftSetStream(plan, s->stream), "cufftSetStream");
+    if (rc != kOk) return rc;
+    timer_begin(&s->timer, 2, s->stream);
+    cufftResult fr = cufftExecC2R(plan, static_cast<cufftComplex*>(s->arranged.ptr), imgs);
+    timer_end(&s->timer, 2, s->stream);
+    rc = check_cufft(fr, "cufftExecC2R (batched)");
+    if (rc != kOk) return rc;
+    if (h_images) {
+        rc = check_cuda(cudaMemcpyAsync(h_images, imgs, per_img * number_of_views * sizeof(float),
+                                        cudaMemcpyDeviceToHost, s->stream),
+                        "images D2H");
+        if (rc != kOk) return rc;
+        return check_cuda(cudaStreamSynchronize(s->stream), "images D2H");
+    }
+    return kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Internal host-side interfaces between the C API layer (mv_api.cu) and the
+// kernel launchers (mv_sum.cu, mv_slice.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace mv {
+
+// Status of an internal call; mirrors enum VisError of meshless_vis_b200.h.
+enum Status : int {
+    kOk = 0,
+    kInvalidValue = 1,
+    kInvalidConfig = 2,
+    kCudaError = 3,
+    kCufftError = 4,
+    kOutOfMemory = 5,
+    kNotRegistered = 6,
+    kUnsupported = 7,
+    kNoKernel = 8,
+};
+
+// Records an error for vis_get_last_error() on this host thread; returns code.
+int set_error(int code, const std::string& message);
+// Maps a CUDA error to a Status and records it (kOk if err == cudaSuccess).
+int check_cuda(cudaError_t err, const char* what);
+
+// An integer lattice of wavenumbers n = (x, y, z), x in [x0, x0+nx), y in
+// [y0, y0+ny), z in [z0, z0+nz).  Sum results are laid out x-major:
+// element ((x - x0) * ny + (y - y0)) * nz + (z - z0)  ("lattice order").
+struct Lattice {
+    int x0, nx;
+    int y0, ny;
+    int z0, nz;
+    // |k| = sqrt((kx x)^2 + (ky y)^2 + (kz z)^2), the argument scale of Phi^.
+    double kx, ky, kz;
+    // Phase in turns of particle p at n: n . (M p), M row-major 3x3.
+    double m[9];
+};
+
+// One group's Fourier sum over a lattice, written to `out` as
+//   out[idx] (=|+=) scale * sum_j w_j Phi^(|k| h_j) exp(-2 pi i n.(M p_j))
+// where idx is lattice order (wrap == 0) or, for the C2R slice layout,
+// ((x < 0 ? x + wrap : x) * row + (y - y0)) with nz == 1.
+struct SumRequest {
+    const float4* particles;  // Constraint AoS
+    const float* radii;       // nullptr: Phi^ evaluated at |k|
+    int n;
+    int basis;
+    Lattice lat;
+    double scale;
+    float2* out;
+    int wrap;
+    int row;
+    bool accumulate;
+    cudaStream_t stream;
+};
+
+// Grow-only device scratch owned by one VisConfig.
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);  // Status
+    void release();
+};
+
+struct KernelTimer;  // per-stage event pairs, see mv_api.cu
+
+// Plain FP32 form.  Uses `ws` for split-K partial sums.
+int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer);
+
+// Slice extraction for a batch of views into the C2R layout
+// [views][nx][ny/2+1].  views: device array of 8 floats per view
+// (u.x, u.y, u.z, v.x, v.y, v.z, step.x, step.y).
+struct SliceRequest {
+    const float2* spectrum;
+    int gx, gy, gz;  // full grid extents Kx, Ky, Kz
+    float inv_step;  // 1 / spectral step
+    const float* views;
+    int number_of_views;
+    int cx, cy;
+    int nx, ny;
+    float2* arranged;
+    cudaStream_t stream;
+};
+int launch_slice_extract(const SliceRequest& req, KernelTimer* timer);
+
+// Per-stage timing hooks (no-ops when timer == nullptr or disabled).
+void timer_begin(KernelTimer* timer, int stage, cudaStream_t stream);
+void timer_end(KernelTimer* timer, int stage, cudaStream_t stream);
+
+int device_sm_count();
+
+// Counts a launch of one of this library's kernels (vis_kernel_launch_count).
+void count_launch();
+
+}  // namespace mv

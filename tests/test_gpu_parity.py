@@ -1,0 +1,231 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the golden
+vectors of the reference's own CPU renderer and against the FP64 oracle.
+
+Tolerances (relative L2 over the whole output):
+  spectra and direct slices vs FP64 ..... 1e-5
+  images cut from the 3D spectrum ....... 1e-4
+  anything vs the reference's FP32 CPU .. 5e-5 (the reference itself is up to
+                                           2.8e-5 off FP64 for Wendland)
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from libmeshlessvis_b200 import meshless as M
+from libmeshlessvis_b200.workloads import c1, constraints, plummer_positions, knn_radius, rotating_views
+
+from util import render_direct, spectrum_and_views, to_dataset
+
+pytestmark = pytest.mark.gpu
+
+SPEC_TOL = 1e-5
+IMAGE_TOL = 1e-4
+REF_TOL = 5e-5
+
+DIRECT = ["b0_xy", "b0_rot", "b0_noradii", "b1_xy", "b1_rot", "b1_noradii", "b2_xy", "b2_rot", "b2_noradii",
+          "two_groups_step01", "timing_test_radii", "timing_test_factor1", "single_particle"]
+SPECTRA = ["spec_b0", "spec_b1", "spec_b2", "spec_b3", "spec_noradii_step05"]
+
+
+@pytest.mark.parametrize("name", DIRECT)
+def test_direct_render_matches_reference_and_fp64(golden, name):
+    c = golden[name]
+    img = render_direct(c["groups"], c["step"], c["cutoff"], c["u"], c["v"], c["samples"])
+    assert O.rel_l2(img, c["fp64_image"]) < SPEC_TOL
+    assert O.rel_l2(img, c["ref_image"]) < REF_TOL
+
+
+@pytest.mark.parametrize("name", SPECTRA)
+@pytest.mark.parametrize("form", [M.FORM_PLAIN, M.FORM_AUTO])
+def test_spectrum_and_views_match_fp64(golden, name, form):
+    c = golden[name]
+    spec, imgs = spectrum_and_views(c["groups"], c["grid"], float(c["step3"]), c["step"], c["cutoff"], c["samples"],
+                                    [tuple(map(tuple, v)) for v in c["views"]], form)
+    assert O.rel_l2(spec, c["fp64_spectrum"]) < SPEC_TOL
+    assert O.rel_l2(imgs, c["fp64_images"]) < IMAGE_TOL
+
+
+def test_c1_full_spectrum_view_and_kat5():
+    """Config C1 in full (N=4096, 64x64x33 half-spectrum, one z-normal view):
+    spectrum vs FP64; the view cut from the spectrum equals the direct render
+    (KAT-5: the z-normal slice lands on lattice points)."""
+    w = c1()
+    spec, imgs = spectrum_and_views(w["groups"], w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"],
+                                    w["views"], M.FORM_PLAIN)
+    ref = O.spectrum_grid(w["groups"], w["step3"], w["grid"])
+    assert O.rel_l2(spec, ref) < SPEC_TOL
+    u, v = w["views"][0]
+    direct = render_direct(w["groups"], w["step"], w["cutoff"], u, v, w["samples"])
+    fp64 = O.render_direct(w["groups"], w["step"], w["cutoff"], u, v, w["samples"])
+    assert O.rel_l2(direct, fp64) < SPEC_TOL
+    assert O.rel_l2(imgs[0], fp64) < SPEC_TOL
+    assert O.rel_l2(imgs[0], direct) < SPEC_TOL
+
+
+def test_c2_shape_wendland_per_particle_h_on_random_points():
+    """C2's particle set (Plummer, 32-NN h and weights, Wendland) at N=65,536
+    on the 128^3 half-spectrum; FP64 check on 1024 random lattice points."""
+    rng = np.random.default_rng(0)
+    n = 65536
+    pos = plummer_positions(rng, n)
+    r32 = knn_radius(pos, 32)
+    wgt = (4.0 / 3.0 * np.pi * r32.astype(np.float64) ** 3 / 32.0).astype(np.float32)  # m / rho, m = 1/N
+    groups = [(constraints(pos, wgt), r32, M.WENDLAND_D3_C2)]
+    spec, _ = spectrum_and_views(groups, (128, 128, 128), 1.0, (1.0, 1.0), (64, 64), (128, 128), None, M.FORM_PLAIN)
+    prng = np.random.default_rng(1)
+    ijk = np.stack([prng.integers(-64, 64, 1024), prng.integers(-64, 64, 1024), prng.integers(0, 65, 1024)], 1)
+    ref = O.spectrum_points(groups[0][0], r32, M.WENDLAND_D3_C2, 1.0, ijk)
+    got = spec[ijk[:, 0] + 64, ijk[:, 1] + 64, ijk[:, 2]]
+    assert O.rel_l2(got, ref) < SPEC_TOL
+
+
+def test_decaying_gaussian_many_groups_large_n_random_points():
+    """16 groups (h-bins) of a log-uniform-h decaying Gaussian set, N=2^18,
+    64^3 lattice; FP64 check on 2048 random points."""
+    rng = np.random.default_rng(2)
+    n = 1 << 18
+    pos = rng.random((n, 3), dtype=np.float32)
+    w = rng.random(n, dtype=np.float32)
+    h = np.exp(rng.uniform(np.log(0.005), np.log(0.05), n)).astype(np.float32)
+    edges = np.exp(np.linspace(np.log(0.005), np.log(0.05), 17))
+    b = np.clip(np.searchsorted(edges, h, side="right") - 1, 0, 15)
+    groups = [(constraints(pos[b == k], w[b == k]), h[b == k], M.GAUSSIAN_DECAYING) for k in range(16)]
+    spec, _ = spectrum_and_views(groups, (64, 64, 64), 1.0, (1.0, 1.0), (32, 32), (64, 64), None, M.FORM_PLAIN)
+    prng = np.random.default_rng(3)
+    ijk = np.stack([prng.integers(-32, 32, 2048), prng.integers(-32, 32, 2048), prng.integers(0, 33, 2048)], 1)
+    ref = sum(O.spectrum_points(g[0], g[1], g[2], 1.0, ijk) for g in groups)
+    got = spec[ijk[:, 0] + 32, ijk[:, 1] + 32, ijk[:, 2]]
+    assert O.rel_l2(got, ref) < SPEC_TOL
+
+
+def test_spectrum_l0_plane_is_hermitian():
+    rng = np.random.default_rng(4)
+    groups = [(constraints(rng.random((999, 3)), rng.standard_normal(999)), np.full(999, 0.03, np.float32), M.SPH)]
+    spec, _ = spectrum_and_views(groups, (32, 32, 32), 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_PLAIN)
+    p = spec[:, :, 0]
+    # F(-i,-j,0) = conj F(i,j,0) for i, j in (-16, 16)
+    a = p[1:, 1:]
+    b = np.conj(p[1:, 1:][::-1, ::-1])
+    assert O.rel_l2(a, b) < 1e-6
+
+
+def test_rotated_views_match_fp64_interpolation():
+    rng = np.random.default_rng(6)
+    groups = [(constraints(rng.random((2000, 3)), rng.standard_normal(2000)),
+               np.exp(rng.uniform(np.log(0.01), np.log(0.04), 2000)).astype(np.float32), M.WENDLAND_D3_C2)]
+    views = rotating_views(12) + [((0.6, 0.8, 0.0), (0.0, 0.0, 1.0)), ((0.0, 0.0, -1.0), (0.0, 1.0, 0.0))]
+    spec, imgs = spectrum_and_views(groups, (32, 32, 32), 1.0, (1.0, 1.0), (16, 16), (32, 32), views, M.FORM_PLAIN)
+    ref_spec = O.spectrum_grid(groups, 1.0, (32, 32, 32))
+    assert O.rel_l2(spec, ref_spec) < SPEC_TOL
+    ref_imgs = O.render_from_spectrum(ref_spec, (32, 32, 32), 1.0, (1.0, 1.0), (16, 16), views, (32, 32))
+    assert O.rel_l2(imgs, ref_imgs) < IMAGE_TOL
+
+
+@pytest.mark.parametrize("n", [0, 1, 255, 257, 4097])
+def test_ragged_and_empty_particle_counts(n):
+    rng = np.random.default_rng(n)
+    groups = [(constraints(rng.random((n, 3)), rng.standard_normal(n)), np.full(n, 0.05, np.float32), M.SPH)]
+    img = render_direct(groups, (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))
+    ref = O.render_direct(groups, (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))
+    if n == 0:
+        assert np.all(img == 0)
+    else:
+        assert O.rel_l2(img, ref) < SPEC_TOL
+    spec, _ = spectrum_and_views(groups, (8, 8, 8), 1.0, (1.0, 1.0), (4, 4), (8, 8), None, M.FORM_PLAIN)
+    ref_s = O.spectrum_grid(groups, 1.0, (8, 8, 8))
+    if n == 0:
+        assert np.all(spec == 0)
+    else:
+        assert O.rel_l2(spec, ref_s) < SPEC_TOL
+
+
+def test_dataset_without_groups_renders_zero():
+    img = render_direct([], (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))
+    assert np.all(img == 0)
+
+
+@pytest.mark.parametrize("cutoff,samples,bl,ps", [((1, 32), (2, 64), 64, 1), ((32, 32), (64, 64), 512, 4),
+                                                   ((24, 8), (48, 16), 128, 3)])
+def test_config_edges_nyquist_and_partial_sums(cutoff, samples, bl, ps):
+    """2cx == Nx (the u-Nyquist column is dropped), tiny cutoffs, several
+    block lengths and partial-sum counts (they change only the padding)."""
+    rng = np.random.default_rng(9)
+    groups = [(constraints(rng.random((700, 3)), rng.standard_normal(700)),
+               np.full(700, 0.02, np.float32), M.GAUSSIAN)]
+    img = render_direct(groups, (1.0, 1.0), cutoff, (1, 0, 0), (0, 1, 0), samples, block_length=bl,
+                        partial_sums=ps)
+    ref = O.render_direct(groups, (1.0, 1.0), cutoff, (1, 0, 0), (0, 1, 0), samples)
+    assert O.rel_l2(img, ref) < SPEC_TOL
+
+
+def test_register_pads_like_the_reference():
+    rng = np.random.default_rng(10)
+    ds = to_dataset([(constraints(rng.random((300, 3)), rng.random(300)), None, M.SPH)])
+    cfg = M.Config(cutoff=(8, 8), samples=(16, 16), block_length=128, partial_sums=3)
+    cfg.register(ds)
+    g = ds.group(0)
+    assert g.d_number_of_terms == 384 and g.d_constraints and not g.d_radii
+    cfg.unregister(ds)
+    cfg.close()
+
+
+def test_invalid_config_and_unregistered_dataset_report_errors():
+    lib = M.lib()
+    cfg = M.Config(cutoff=(40, 8), samples=(64, 16), block_length=64)  # 2*40*8 % 64 != 0
+    assert not cfg.check()
+    ds = to_dataset([(constraints(np.zeros((4, 3)), np.ones(4)), None, M.SPH)])
+    lib.vis_fourier_volume_rendering(ds.ref, cfg.ptr)
+    assert lib.vis_get_last_error() == 2
+    lib.vis_clear_last_error()
+    cfg.close()
+    cfg = M.Config(cutoff=(8, 8), samples=(16, 16), block_length=64)
+    lib.vis_fourier_volume_rendering(ds.ref, cfg.ptr)
+    assert lib.vis_get_last_error() == 6
+    lib.vis_clear_last_error()
+    cfg.close()
+
+
+def test_repeat_render_is_deterministic():
+    rng = np.random.default_rng(12)
+    groups = [(constraints(rng.random((5000, 3)), rng.standard_normal(5000)),
+               np.full(5000, 0.02, np.float32), M.WENDLAND_D3_C2)]
+    cfg = M.Config(cutoff=(16, 16), samples=(32, 32), block_length=64)
+    ds = to_dataset(groups)
+    cfg.register(ds)
+    cfg.render(ds)
+    a = cfg.image()
+    cfg.render(ds)
+    b = cfg.image()
+    cfg.unregister(ds)
+    cfg.close()
+    np.testing.assert_array_equal(a, b)
+
+
+def test_manual_d_image_stream_and_timing():
+    """A caller-owned device image (the headless stand-in for the reference's
+    GL pixel buffer) on a caller-owned stream, with per-stage timing."""
+    import torch
+
+    lib = M.lib()
+    rng = np.random.default_rng(13)
+    groups = [(constraints(rng.random((1000, 3)), rng.standard_normal(1000)), np.full(1000, 0.03, np.float32),
+               M.SPH)]
+    cfg = M.Config(cutoff=(8, 8), samples=(16, 16), block_length=64, automatic_d_image=False)
+    buf = torch.zeros((16, 16), dtype=torch.float32, device="cuda")
+    lib.vis_config_manual_d_image(cfg.ptr, buf.data_ptr())
+    stream = torch.cuda.Stream()
+    cfg.set_stream(stream.cuda_stream)
+    ds = to_dataset(groups)
+    cfg.register(ds)
+    cfg.enable_timing(True)
+    cfg.render(ds)
+    cfg.synchronize()
+    img = buf.cpu().numpy()
+    ms, launches = cfg.kernel_time(M.STAGE_SUM)
+    assert launches == 1 and ms > 0
+    ms_fft, launches_fft = cfg.kernel_time(M.STAGE_FFT)
+    assert launches_fft == 1
+    cfg.unregister(ds)
+    cfg.close()
+    ref = O.render_direct(groups, (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))
+    assert O.rel_l2(img, ref) < SPEC_TOL
