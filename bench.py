@@ -46,7 +46,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c3"], default="c2")
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3"], default="c2",
+                   help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views (profiling case)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -60,6 +61,10 @@ def workload(name):
         return W.c1()
     if name == "c3":
         return W.c3()
+    if name == "c2s":
+        w = W.c2(n=65536, grid=64, views=16)
+        w["name"] = "C2-small"
+        return w
     return W.c2()
 
 

@@ -13,6 +13,7 @@
 //     host-image variant of vis_spectrum_render_views wait for it.
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -72,8 +73,17 @@ int device_sm_count() {
 
 namespace {
 std::atomic<unsigned long long> g_launches{0};
-}
+std::mutex g_radii_mu;
+std::unordered_map<const float*, float> g_radius_max;
+}  // namespace
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+float registered_radius_max(const float* d_radii) {
+    if (!d_radii) return -1.f;
+    std::lock_guard<std::mutex> lock(g_radii_mu);
+    auto it = g_radius_max.find(d_radii);
+    return it == g_radius_max.end() ? -1.f : it->second;
+}
 
 // --------------------------------------------------------------- workspace
 int Workspace::reserve(size_t need) {
@@ -468,6 +478,12 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
                         cudaMemcpyHostToDevice, s->stream);
         if (grp.h_radii) {
             if (device_alloc(&grp.d_radii, (size_t)padded) != kOk) return;
+            float hmax = 0.f;
+            for (int k = 0; k < grp.number_of_terms; ++k) hmax = std::max(hmax, std::fabs(grp.h_radii[k]));
+            {
+                std::lock_guard<std::mutex> lock(g_radii_mu);
+                g_radius_max[grp.d_radii] = hmax;
+            }
             cudaMemsetAsync(grp.d_radii, 0, sizeof(float) * padded, s->stream);
             cudaMemcpyAsync(grp.d_radii, grp.h_radii, sizeof(float) * grp.number_of_terms, cudaMemcpyHostToDevice,
                             s->stream);
@@ -486,6 +502,10 @@ void vis_unregister_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
     cudaStreamSynchronize(s->stream);
     for (int g = 0; g < ds->number_of_groups; ++g) {
         cudaFree(ds->groups[g].d_constraints);
+        if (ds->groups[g].d_radii) {
+            std::lock_guard<std::mutex> lock(g_radii_mu);
+            g_radius_max.erase(ds->groups[g].d_radii);
+        }
         cudaFree(ds->groups[g].d_radii);
         ds->groups[g].d_constraints = nullptr;
         ds->groups[g].d_radii = nullptr;
@@ -528,6 +548,7 @@ void vis_fourier_volume_rendering(MeshlessDataset* ds, VisConfig* c) {
         SumRequest r{};
         r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
         r.radii = grp.d_radii;
+        r.radius_max = registered_radius_max(grp.d_radii);
         r.n = grp.number_of_terms;
         r.basis = (int)grp.basis_function_id;
         // Slice x in (-cx, cx): the reference also evaluates x == cx
@@ -663,6 +684,7 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
         SumRequest r{};
         r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
         r.radii = grp.d_radii;
+        r.radius_max = registered_radius_max(grp.d_radii);
         r.n = grp.number_of_terms;
         r.basis = (int)grp.basis_function_id;
         r.lat.x0 = -sp->grid.x / 2;

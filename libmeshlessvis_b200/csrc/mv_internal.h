@@ -48,6 +48,7 @@ struct Lattice {
 struct SumRequest {
     const float4* particles;  // Constraint AoS
     const float* radii;       // nullptr: Phi^ evaluated at |k|
+    float radius_max;         // largest radius if known (registration), else < 0
     int n;
     int basis;
     Lattice lat;
@@ -93,6 +94,10 @@ void timer_begin(KernelTimer* timer, int stage, cudaStream_t stream);
 void timer_end(KernelTimer* timer, int stage, cudaStream_t stream);
 
 int device_sm_count();
+
+// Largest radius of a registered group, keyed by its device radii pointer
+// (recorded by vis_register_meshless_dataset); -1 if unknown.
+float registered_radius_max(const float* d_radii);
 
 // Counts a launch of one of this library's kernels (vis_kernel_launch_count).
 void count_launch();

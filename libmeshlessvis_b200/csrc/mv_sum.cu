@@ -9,17 +9,30 @@
 // 80-83), each split writing FP32 partial sums to a workspace that the
 // finalize kernel reduces in FP64.
 //
-// Per particle tile (256 particles staged in shared memory by the block), the
-// loader converts each position to fixed-point turns per lattice axis,
-// Q_a = round(2^32 (M p)_a) mod 2^32, in FP64.  The phase of a term is then the
-// exact integer x Qx + y Qy + z Qz mod 2^32 (wrapping 32-bit multiply-add),
-// converted to radians in [-pi, pi) and passed to the SFU sincos.  The
-// reference instead forms 2 pi f.x in FP32 and calls __sincosf on an
-// unreduced argument (fourier_transform.cu:125), whose error grows with |f.x|.
+// Phase.  Per particle tile (256 particles staged in shared memory by the
+// block) the loader converts each position to fixed-point turns per lattice
+// axis, Q_a = round(2^32 (M p)_a) mod 2^32, in FP64, and the x-step rotation
+// R = exp(2 pi i Qx / 2^32) with an FP64 sincospi.  A thread forms the exact
+// integer phase of its first term, x0 Qx + y Qy + z Qz mod 2^32 (wrapping
+// 32-bit multiply-add), takes one SFU sincos of it, and reaches its other L-1
+// terms by complex multiplication with R.  The reference instead forms
+// 2 pi f.x in FP32 and calls __sincosf per term on an unreduced argument
+// (fourier_transform.cu:125), whose error grows with |f.x|.
 //
-// Accumulation: each tile's 256 terms are summed in FP32 registers and the
-// tile sums are added with Kahan compensation; splits are reduced in FP64.
+// Amplitude w_j Phi^(|k| h_j):
+//   - groups without radii: Phi^(|k|) is applied per frequency in FP64 by the
+//     finalize kernel (it does not depend on the particle);
+//   - SPH / Wendland with radii: Phi^ is read from a shared-memory table of
+//     cubic pieces on node-centred cells of width ds (a branch point of the
+//     reference's piecewise definition falls on a cell boundary), built per
+//     launch in FP64 by phi_table_kernel; max error ~1.1e-7 of Phi^(0); terms
+//     beyond the table evaluate the accurate FP32 form directly;
+//   - Gaussians with radii: exp2 per term.
+//
+// Accumulation: each tile's terms are summed in FP32 registers and the tile
+// sums are added with Kahan compensation; splits are reduced in FP64.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 
 #include "mv_device.cuh"
@@ -30,6 +43,15 @@ namespace mv {
 namespace {
 
 constexpr int kThreads = 256;  // threads per block == particles per tile
+constexpr int kMaxTable = 4096;  // cubic cells held in shared memory (64 KB)
+
+// kAmpGaussRec: decaying Gaussian exp(-pi h^2 |k|^2) factored as
+// exp(-pi h^2 (y^2+z^2)) (one exp2 per particle and thread) times the x factor
+// g(x) = exp(-pi h^2 x^2), advanced along the thread's L terms by
+// g(x+1) = g(x) q(x), q(x+1) = q(x) exp(-2 pi h^2).  An x factor that
+// underflows FP32 stays below 1e-28 over 8 steps, so nothing significant is
+// lost.
+enum Amp : int { kAmpFactored = 0, kAmpTable = 1, kAmpExp2 = 2, kAmpGaussRec = 3 };
 
 struct SumKernelArgs {
     const float4* particles;
@@ -40,14 +62,24 @@ struct SumKernelArgs {
     int nxc;     // number of x chunks of L
     int n_rest;  // ny * nz
     float2* partial;  // [split][nxc * L][n_rest]
+    const float4* table;  // cubic cells (kAmpTable); cell table_n is all zero
+    int table_n;
+    float inv_ds;  // 1 / cell width (kAmpTable)
+    float amp_scale;  // kAmpExp2: +-pi log2(e)
 };
 
-template <int L, int BASIS, bool FACTORED>
-__global__ void __launch_bounds__(kThreads) plain_sum_kernel(SumKernelArgs a) {
-    __shared__ uint4 s_q[kThreads];  // Qx, Qy, Qz, weight bits
-    __shared__ float s_h[kThreads];
+template <int L, int BASIS, int AMP>
+__global__ void __launch_bounds__(kThreads, 2) plain_sum_kernel(SumKernelArgs a) {
+    extern __shared__ float4 s_tab[];  // table cells (kAmpTable only)
+    __shared__ uint4 s_q[kThreads];    // Qx, Qy, Qz, weight bits
+    __shared__ float2 s_rot[kThreads];  // exp(2 pi i Qx / 2^32)
+    __shared__ float s_h[kThreads];    // per-particle amplitude parameter
 
     const int tid = threadIdx.x;
+    if constexpr (AMP == kAmpTable) {
+        for (int i = tid; i <= a.table_n; i += kThreads) s_tab[i] = a.table[i];
+    }
+
     const long long t = (long long)blockIdx.x * kThreads + tid;
     const bool active = t < (long long)a.nxc * a.n_rest;
     const int xc = active ? (int)(t / a.n_rest) : 0;
@@ -56,13 +88,23 @@ __global__ void __launch_bounds__(kThreads) plain_sum_kernel(SumKernelArgs a) {
     const int z = a.lat.z0 + rest % a.lat.nz;
     const int xb = a.lat.x0 + xc * L;
 
+    // |k| (kAmpTable) or |k|^2 (kAmpExp2) of the thread's L terms.
     float r[L];
-    if constexpr (!FACTORED) {
+    float ryz2 = 0.f;  // kAmpGaussRec: (ky y)^2 + (kz z)^2
+    if constexpr (AMP == kAmpGaussRec) {
+        const double ry = a.lat.ky * y, rz = a.lat.kz * z;
+        ryz2 = (float)(ry * ry + rz * rz);
+        const double rx = a.lat.kx * xb;
+        r[0] = (float)(rx * rx);                            // (kx x0)^2
+        r[1] = (float)(a.lat.kx * a.lat.kx * (2.0 * xb + 1));  // exponent of q(x0), per unit -pi h^2
+        r[2] = (float)(2.0 * a.lat.kx * a.lat.kx);             // exponent of q's ratio
+    } else if constexpr (AMP != kAmpFactored) {
         const double ry = a.lat.ky * y, rz = a.lat.kz * z;
 #pragma unroll
         for (int m = 0; m < L; ++m) {
             const double rx = a.lat.kx * (xb + m);
-            r[m] = (float)sqrt(rx * rx + ry * ry + rz * rz);
+            const double r2 = rx * rx + ry * ry + rz * rz;
+            r[m] = AMP == kAmpTable ? (float)sqrt(r2) : (float)r2;
         }
     }
 
@@ -84,10 +126,17 @@ __global__ void __launch_bounds__(kThreads) plain_sum_kernel(SumKernelArgs a) {
             const float4 p = a.particles[idx];
             const double px = p.x, py = p.y, pz = p.z;
             const double* m = a.lat.m;
-            s_q[tid] = make_uint4(fixed_turns(m[0] * px + m[1] * py + m[2] * pz),
-                                  fixed_turns(m[3] * px + m[4] * py + m[5] * pz),
+            const uint32_t qx = fixed_turns(m[0] * px + m[1] * py + m[2] * pz);
+            s_q[tid] = make_uint4(qx, fixed_turns(m[3] * px + m[4] * py + m[5] * pz),
                                   fixed_turns(m[6] * px + m[7] * py + m[8] * pz), __float_as_uint(p.w));
-            s_h[tid] = FACTORED ? 0.f : a.radii[idx];
+            double sn, cs;
+            sincospi((double)(int32_t)qx * (1.0 / 2147483648.0), &sn, &cs);
+            s_rot[tid] = make_float2((float)cs, (float)sn);
+            if constexpr (AMP == kAmpTable) s_h[tid] = a.radii[idx] * a.inv_ds;
+            else if constexpr (AMP == kAmpExp2 || AMP == kAmpGaussRec) {
+                const float h = a.radii[idx];
+                s_h[tid] = a.amp_scale * h * h;
+            }
         }
         __syncthreads();
         const int cnt = min(kThreads, end - t0);
@@ -96,21 +145,58 @@ __global__ void __launch_bounds__(kThreads) plain_sum_kernel(SumKernelArgs a) {
 #pragma unroll
         for (int m = 0; m < L; ++m) acc[m] = make_float2(0.f, 0.f);
 
+#pragma unroll 2
         for (int j = 0; j < cnt; ++j) {
             const uint4 q = s_q[j];
-            const float w = __uint_as_float(q.w);
-            uint32_t ph = ux * q.x + uy * q.y + uz * q.z;
-            float h = 0.f;
-            if constexpr (!FACTORED) h = s_h[j];
+            const float2 R = s_rot[j];
+            float hv = 0.f;
+            if constexpr (AMP != kAmpFactored) hv = s_h[j];
+            const uint32_t ph = ux * q.x + uy * q.y + uz * q.z;
+            float sn, cs;
+            __sincosf(turns_to_radians(ph), &sn, &cs);
+            float w = __uint_as_float(q.w);
+            float Rx = R.x, Ry = R.y, qc = 1.f;
+            if constexpr (AMP == kAmpGaussRec) {
+                // hv = -pi log2(e) h^2
+                w *= exp2f(hv * (ryz2 + r[0]));
+                const float q0 = exp2f(hv * r[1]);
+                qc = exp2f(hv * r[2]);
+                Rx *= q0;
+                Ry *= q0;
+            }
+            float zr = w * cs, zi = w * sn;
 #pragma unroll
             for (int m = 0; m < L; ++m) {
-                float sn, cs;
-                __sincosf(turns_to_radians(ph), &sn, &cs);
-                float amp = w;
-                if constexpr (!FACTORED) amp *= phi<BASIS>(r[m] * h);
-                acc[m].x = fmaf(amp, cs, acc[m].x);
-                acc[m].y = fmaf(amp, sn, acc[m].y);
-                ph += q.x;
+                if constexpr (AMP == kAmpFactored || AMP == kAmpGaussRec) {
+                    acc[m].x += zr;
+                    acc[m].y += zi;
+                } else {
+                    float amp;
+                    if constexpr (AMP == kAmpTable) {
+                        const float u = r[m] * hv;  // s / ds
+                        const float tt = u + 12582912.0f;  // round to nearest cell (1.5 * 2^23)
+                        // beyond the table (and for negative radii) the last,
+                        // all-zero cell is used
+                        const unsigned k = min((unsigned)(__float_as_int(tt) - 0x4B400000), (unsigned)a.table_n);
+                        const float fr = u - (tt - 12582912.0f);
+                        const float4 c = s_tab[k];
+                        amp = fmaf(fmaf(fmaf(c.w, fr, c.z), fr, c.y), fr, c.x);
+                    } else {
+                        amp = exp2f(hv * r[m]);
+                    }
+                    acc[m].x = fmaf(amp, zr, acc[m].x);
+                    acc[m].y = fmaf(amp, zi, acc[m].y);
+                }
+                if (m + 1 < L) {
+                    const float nr = fmaf(zr, Rx, -zi * Ry);
+                    const float ni = fmaf(zr, Ry, zi * Rx);
+                    zr = nr;
+                    zi = ni;
+                    if constexpr (AMP == kAmpGaussRec) {
+                        Rx *= qc;
+                        Ry *= qc;
+                    }
+                }
             }
         }
         // Kahan: add this tile's sums to the running totals.
@@ -132,6 +218,43 @@ __global__ void __launch_bounds__(kThreads) plain_sum_kernel(SumKernelArgs a) {
     float2* out = a.partial + blockIdx.y * plane + (size_t)(xc * L) * a.n_rest + rest;
 #pragma unroll
     for (int m = 0; m < L; ++m) out[(size_t)m * a.n_rest] = make_float2(tot[m].x - comp[m].x, tot[m].y - comp[m].y);
+}
+
+// Cubic pieces of Phi^ on cells [(k - 1/2) ds, (k + 1/2) ds]: the polynomial in
+// fr = s/ds - k interpolating Phi^ (FP64, reference branch points) at the four
+// Chebyshev points of the cell.  Cells never straddle a branch point because
+// ds is chosen so that each branch point is a half-integer multiple of ds.
+__global__ void phi_table_kernel(int basis, double ds, int n, float4* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > n) return;
+    if (k == n) {
+        out[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    double x[4], f[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        x[i] = 0.5 * cospi((2 * i + 1) / 8.0);
+        f[i] = phi_fp64(basis, (k + x[i]) * ds);
+    }
+    // Newton divided differences, then expansion to monomials in fr.
+    double d[4] = {f[0], f[1], f[2], f[3]};
+    for (int lvl = 1; lvl < 4; ++lvl)
+        for (int i = 3; i >= lvl; --i) d[i] = (d[i] - d[i - 1]) / (x[i] - x[i - lvl]);
+    double c[4] = {d[3], 0.0, 0.0, 0.0};  // Horner-style expansion of the Newton form
+    int deg = 0;
+    for (int i = 2; i >= 0; --i) {
+        // c(x) = c(x) * (x - x[i]) + d[i]
+        double nc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int p = 0; p <= deg; ++p) {
+            nc[p + 1] += c[p];
+            nc[p] -= x[i] * c[p];
+        }
+        ++deg;
+        nc[0] += d[i];
+        for (int p = 0; p < 4; ++p) c[p] = nc[p];
+    }
+    out[k] = make_float4((float)c[0], (float)c[1], (float)c[2], (float)c[3]);
 }
 
 struct FinalizeArgs {
@@ -186,16 +309,27 @@ __global__ void finalize_kernel(FinalizeArgs f) {
 
 using SumKernel = void (*)(SumKernelArgs);
 
+template <int L, int BASIS>
+SumKernel pick_amp(int amp) {
+    if (amp == kAmpFactored) return plain_sum_kernel<L, BASIS, kAmpFactored>;
+    if constexpr (BASIS == kSph || BASIS == kWendland) return plain_sum_kernel<L, BASIS, kAmpTable>;
+    else if constexpr (BASIS == kGaussianDecaying && L > 1) return plain_sum_kernel<L, BASIS, kAmpGaussRec>;
+    else return plain_sum_kernel<L, BASIS, kAmpExp2>;
+}
+
 template <int L>
-SumKernel pick(int basis, bool factored) {
+SumKernel pick(int basis, int amp) {
     switch (basis) {
-    case kSph: return factored ? plain_sum_kernel<L, kSph, true> : plain_sum_kernel<L, kSph, false>;
-    case kGaussian: return factored ? plain_sum_kernel<L, kGaussian, true> : plain_sum_kernel<L, kGaussian, false>;
-    case kWendland: return factored ? plain_sum_kernel<L, kWendland, true> : plain_sum_kernel<L, kWendland, false>;
-    default:
-        return factored ? plain_sum_kernel<L, kGaussianDecaying, true> : plain_sum_kernel<L, kGaussianDecaying, false>;
+    case kSph: return pick_amp<L, kSph>(amp);
+    case kGaussian: return pick_amp<L, kGaussian>(amp);
+    case kWendland: return pick_amp<L, kWendland>(amp);
+    default: return pick_amp<L, kGaussianDecaying>(amp);
     }
 }
+
+// Table cell width: a branch point of the reference's piecewise Phi^ (0.06f
+// for SPH, 0.24f for Wendland) sits at (K + 1/2) ds.
+double table_cell(int basis) { return basis == kSph ? (double)0.06f / 3.5 : (double)0.24f / 15.5; }
 
 }  // namespace
 
@@ -207,24 +341,45 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     if (req.n > 0 && req.particles == nullptr) return set_error(kInvalidValue, "dataset group has no device particles");
 
     const bool factored = req.radii == nullptr;
-    const int L = lat.nx >= 16 ? 4 : 1;
+    const int amp = factored ? kAmpFactored
+                    : (req.basis == kSph || req.basis == kWendland) ? kAmpTable
+                                                                      : kAmpExp2;
+    const int L = lat.nx >= 8 ? 8 : 1;
     const int nxc = (lat.nx + L - 1) / L;
     const long long n_rest = (long long)lat.ny * lat.nz;
     const long long threads = (long long)nxc * n_rest;
     if (threads > (1LL << 31) - 1) return set_error(kInvalidValue, "lattice too large");
     const long long blocks_f = (threads + kThreads - 1) / kThreads;
 
-    // Split the particle range until the grid holds ~8 blocks per SM, keeping
-    // at least 4 tiles of particles per split.
-    const long long target = (long long)device_sm_count() * 8;
+    // Split the particle range until the grid holds ~6 blocks per SM (two
+    // waves of the 3 resident blocks), keeping at least 4 tiles per split.
+    const long long target = (long long)device_sm_count() * 6;
     long long max_splits = std::max<long long>(1, (req.n + 4 * kThreads - 1) / (4 * kThreads));
     long long splits = std::min<long long>(std::max<long long>(1, (target + blocks_f - 1) / blocks_f), max_splits);
     splits = std::min<long long>(splits, 65535);
     long long chunk = req.n > 0 ? ((req.n + splits - 1) / splits + kThreads - 1) / kThreads * kThreads : kThreads;
     splits = req.n > 0 ? (req.n + chunk - 1) / chunk : 1;
 
+    // Table size: cells up to the largest s = |k|max * hmax (when known).
+    int table_n = 0;
+    double ds = 0.0;
+    if (amp == kAmpTable) {
+        ds = table_cell(req.basis);
+        const double kx = std::fabs(lat.kx) * std::max(std::abs(lat.x0), std::abs(lat.x0 + lat.nx - 1));
+        const double ky = std::fabs(lat.ky) * std::max(std::abs(lat.y0), std::abs(lat.y0 + lat.ny - 1));
+        const double kz = std::fabs(lat.kz) * std::max(std::abs(lat.z0), std::abs(lat.z0 + lat.nz - 1));
+        const double rmax = std::sqrt(kx * kx + ky * ky + kz * kz);
+        const double smax = req.radius_max >= 0.f ? rmax * req.radius_max : 1e30;
+        // Beyond kMaxTable cells (s > 63 for Wendland, > 60 for SPH) |Phi^| < 1e-11
+        // and the zero cell stands in for it.
+        table_n = (int)std::min<double>(kMaxTable, std::ceil(smax / ds) + 2.0);
+        table_n = std::max(table_n, 1);
+    }
+
     const size_t plane = (size_t)nxc * L * n_rest;
-    int st = ws.reserve(plane * splits * sizeof(float2));
+    const size_t part_bytes = (plane * splits * sizeof(float2) + 255) / 256 * 256;
+    const size_t table_cells = amp == kAmpTable ? (size_t)table_n + 1 : 0;
+    int st = ws.reserve(part_bytes + table_cells * sizeof(float4));
     if (st != kOk) return st;
 
     SumKernelArgs a;
@@ -236,10 +391,26 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     a.nxc = nxc;
     a.n_rest = (int)n_rest;
     a.partial = static_cast<float2*>(ws.ptr);
+    a.table = reinterpret_cast<const float4*>(static_cast<char*>(ws.ptr) + part_bytes);
+    a.table_n = table_n;
+    a.inv_ds = ds > 0 ? (float)(1.0 / ds) : 0.f;
+    a.amp_scale = req.basis == kGaussian ? kPiLog2e : -kPiLog2e;
 
-    SumKernel k = (L == 4) ? pick<4>(req.basis, factored) : pick<1>(req.basis, factored);
+    if (amp == kAmpTable) {
+        phi_table_kernel<<<(table_n + 128) / 128, 128, 0, req.stream>>>(req.basis, ds, table_n,
+                                                                         const_cast<float4*>(a.table));
+        count_launch();
+    }
+
+    SumKernel k = (L == 8) ? pick<8>(req.basis, amp) : pick<1>(req.basis, amp);
+    const size_t dyn_smem = table_cells * sizeof(float4);
+    if (dyn_smem > 48 * 1024) {
+        st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
+                        "cudaFuncSetAttribute");
+        if (st != kOk) return st;
+    }
     timer_begin(timer, 0, req.stream);
-    k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, 0, req.stream>>>(a);
+    k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, dyn_smem, req.stream>>>(a);
     count_launch();
     timer_end(timer, 0, req.stream);
     st = check_cuda(cudaGetLastError(), "plain_sum_kernel launch");
