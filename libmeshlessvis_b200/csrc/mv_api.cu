@@ -73,16 +73,16 @@ int device_sm_count() {
 
 namespace {
 std::atomic<unsigned long long> g_launches{0};
-std::mutex g_radii_mu;
-std::unordered_map<const float*, float> g_radius_max;
+std::mutex g_stats_mu;
+std::unordered_map<const void*, GroupStats> g_stats;
 }  // namespace
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-float registered_radius_max(const float* d_radii) {
-    if (!d_radii) return -1.f;
-    std::lock_guard<std::mutex> lock(g_radii_mu);
-    auto it = g_radius_max.find(d_radii);
-    return it == g_radius_max.end() ? -1.f : it->second;
+GroupStats registered_group_stats(const void* d_constraints) {
+    if (!d_constraints) return GroupStats{};
+    std::lock_guard<std::mutex> lock(g_stats_mu);
+    auto it = g_stats.find(d_constraints);
+    return it == g_stats.end() ? GroupStats{} : it->second;
 }
 
 // --------------------------------------------------------------- workspace
@@ -171,6 +171,8 @@ struct ConfigState {
     Workspace arranged;  // batched C2R inputs of vis_spectrum_render_views
     Workspace images;    // library-owned batched images
     Workspace views;     // per-view parameters
+    Workspace acc64;     // FP64 accumulators of the tensor-core form
+    Workspace error_word;  // device int set by kernels that give up a bounded wait
     std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
     KernelTimer timer;
 
@@ -180,6 +182,8 @@ struct ConfigState {
         arranged.release();
         images.release();
         views.release();
+        acc64.release();
+        error_word.release();
         for (auto& kv : batched_plans) cufftDestroy(kv.second);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -299,6 +303,8 @@ VisConfig* vis_config_create(bool automatic_d_image, float2 step_size, int2 cuto
     ConfigState* s = new ConfigState();
     int st = check_cuda(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     s->own_stream = st == kOk;
+    if (st == kOk) st = s->error_word.reserve(256);
+    if (st == kOk) st = check_cuda(cudaMemset(s->error_word.ptr, 0, 256), "cudaMemset");
     if (st == kOk) st = device_alloc(&c->_d_freq_image, freq_image_count(c));
     if (st == kOk) st = device_alloc(&c->_d_freq_image_arranged, arranged_count(c));
     if (st == kOk && automatic_d_image) st = device_alloc(&c->_d_image, image_count(c));
@@ -441,10 +447,26 @@ cudaStream_t vis_config_get_stream(VisConfig* c) {
     return s->stream;
 }
 
+// Waits for the config's stream and reports a kernel that gave up one of its
+// bounded waits (the word is cleared once reported).
+static int sync_and_check(ConfigState* s, const char* what) {
+    int rc = check_cuda(cudaStreamSynchronize(s->stream), what);
+    if (rc != kOk) return rc;
+    int word = 0;
+    rc = check_cuda(cudaMemcpy(&word, s->error_word.ptr, sizeof(int), cudaMemcpyDeviceToHost), what);
+    if (rc != kOk) return rc;
+    if (word != 0) {
+        cudaMemset(s->error_word.ptr, 0, sizeof(int));
+        return set_error(kCudaError, std::string(what) + ": a tensor-core kernel timed out in a bounded wait (code " +
+                                         std::to_string(word) + "); its results are invalid");
+    }
+    return kOk;
+}
+
 int vis_config_synchronize(VisConfig* c) {
     ConfigState* s = c ? state_of(c) : nullptr;
     if (!s) return set_error(kInvalidValue, "vis_config_synchronize: unknown config");
-    return check_cuda(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize");
+    return sync_and_check(s, "vis_config_synchronize");
 }
 
 // meshless_vis/meshless_vis.cu:264-290: device copies padded with zeros to a
@@ -476,14 +498,23 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         cudaMemsetAsync(grp.d_constraints, 0, sizeof(Constraint) * padded, s->stream);
         cudaMemcpyAsync(grp.d_constraints, grp.h_constraints, sizeof(Constraint) * grp.number_of_terms,
                         cudaMemcpyHostToDevice, s->stream);
+        GroupStats gs;
+        gs.weight_max = 0.f;
+        for (int k = 0; k < grp.number_of_terms; ++k)
+            gs.weight_max = std::max(gs.weight_max, std::fabs(grp.h_constraints[k].weight));
+        if (grp.h_radii && grp.number_of_terms > 0) {
+            gs.radius_min = gs.radius_max = grp.h_radii[0];
+            for (int k = 1; k < grp.number_of_terms; ++k) {
+                gs.radius_min = std::min(gs.radius_min, grp.h_radii[k]);
+                gs.radius_max = std::max(gs.radius_max, grp.h_radii[k]);
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lock(g_stats_mu);
+            g_stats[grp.d_constraints] = gs;
+        }
         if (grp.h_radii) {
             if (device_alloc(&grp.d_radii, (size_t)padded) != kOk) return;
-            float hmax = 0.f;
-            for (int k = 0; k < grp.number_of_terms; ++k) hmax = std::max(hmax, std::fabs(grp.h_radii[k]));
-            {
-                std::lock_guard<std::mutex> lock(g_radii_mu);
-                g_radius_max[grp.d_radii] = hmax;
-            }
             cudaMemsetAsync(grp.d_radii, 0, sizeof(float) * padded, s->stream);
             cudaMemcpyAsync(grp.d_radii, grp.h_radii, sizeof(float) * grp.number_of_terms, cudaMemcpyHostToDevice,
                             s->stream);
@@ -502,9 +533,9 @@ void vis_unregister_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
     cudaStreamSynchronize(s->stream);
     for (int g = 0; g < ds->number_of_groups; ++g) {
         cudaFree(ds->groups[g].d_constraints);
-        if (ds->groups[g].d_radii) {
-            std::lock_guard<std::mutex> lock(g_radii_mu);
-            g_radius_max.erase(ds->groups[g].d_radii);
+        if (ds->groups[g].d_constraints) {
+            std::lock_guard<std::mutex> lock(g_stats_mu);
+            g_stats.erase(ds->groups[g].d_constraints);
         }
         cudaFree(ds->groups[g].d_radii);
         ds->groups[g].d_constraints = nullptr;
@@ -548,7 +579,13 @@ void vis_fourier_volume_rendering(MeshlessDataset* ds, VisConfig* c) {
         SumRequest r{};
         r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
         r.radii = grp.d_radii;
-        r.radius_max = registered_radius_max(grp.d_radii);
+        {
+            const GroupStats gs = registered_group_stats(grp.d_constraints);
+            r.radius_min = gs.radius_min;
+            r.radius_max = gs.radius_max;
+            r.weight_max = gs.weight_max;
+        }
+        r.error_flag = static_cast<int*>(s->error_word.ptr);
         r.n = grp.number_of_terms;
         r.basis = (int)grp.basis_function_id;
         // Slice x in (-cx, cx): the reference also evaluates x == cx
@@ -636,7 +673,7 @@ struct VisSpectrum {
 
 namespace mv {
 int tensor_sum_available(const SumRequest& req);  // mv_tc_sum.cu
-int launch_tensor_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer);
+int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, KernelTimer* timer);
 }  // namespace mv
 
 extern "C" {
@@ -684,7 +721,13 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
         SumRequest r{};
         r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
         r.radii = grp.d_radii;
-        r.radius_max = registered_radius_max(grp.d_radii);
+        {
+            const GroupStats gs = registered_group_stats(grp.d_constraints);
+            r.radius_min = gs.radius_min;
+            r.radius_max = gs.radius_max;
+            r.weight_max = gs.weight_max;
+        }
+        r.error_flag = static_cast<int*>(s->error_word.ptr);
         r.n = grp.number_of_terms;
         r.basis = (int)grp.basis_function_id;
         r.lat.x0 = -sp->grid.x / 2;
@@ -699,13 +742,17 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
         std::memcpy(r.lat.m, m, sizeof(m));
         r.scale = 1.0;
         r.out = sp->data;
+        r.out_base = 0;
+        r.out_sx = (long long)sp->grid.y * (sp->grid.z / 2 + 1);
+        r.out_sy = sp->grid.z / 2 + 1;
+        r.out_sz = 1;
         r.wrap = 0;
         r.row = 0;
         r.accumulate = g > 0;
         r.stream = s->stream;
         int rc;
         const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
-        if (want_tc && tensor_sum_available(r)) rc = launch_tensor_sum(r, s->partials, &s->timer);
+        if (want_tc && tensor_sum_available(r)) rc = launch_tensor_sum(r, s->partials, s->acc64, &s->timer);
         else rc = launch_plain_sum(r, s->partials, &s->timer);
         if (rc != kOk) return rc;
     }
@@ -718,7 +765,7 @@ int vis_spectrum_copy_to_host(VisSpectrum* sp, VisConfig* c, float2* h) {
     int rc = check_cuda(cudaMemcpyAsync(h, sp->data, sizeof(float2) * sp->count, cudaMemcpyDeviceToHost, s->stream),
                         "vis_spectrum_copy_to_host");
     if (rc != kOk) return rc;
-    return check_cuda(cudaStreamSynchronize(s->stream), "vis_spectrum_copy_to_host");
+    return sync_and_check(s, "vis_spectrum_copy_to_host");
 }
 
 int vis_spectrum_render_views(VisSpectrum* sp, VisConfig* c, int number_of_views, const float3* u_axes,
@@ -796,7 +843,7 @@ int vis_spectrum_render_views(VisSpectrum* sp, VisConfig* c, int number_of_views
                                         cudaMemcpyDeviceToHost, s->stream),
                         "images D2H");
         if (rc != kOk) return rc;
-        return check_cuda(cudaStreamSynchronize(s->stream), "images D2H");
+        return sync_and_check(s, "vis_spectrum_render_views");
     }
     return kOk;
 }

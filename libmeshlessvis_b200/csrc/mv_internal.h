@@ -43,21 +43,26 @@ struct Lattice {
 
 // One group's Fourier sum over a lattice, written to `out` as
 //   out[idx] (=|+=) scale * sum_j w_j Phi^(|k| h_j) exp(-2 pi i n.(M p_j))
-// where idx is lattice order (wrap == 0) or, for the C2R slice layout,
+// where idx = out_base + (x-x0) out_sx + (y-y0) out_sy + (z-z0) out_sz
+// (wrap == 0) or, for the C2R slice layout,
 // ((x < 0 ? x + wrap : x) * row + (y - y0)) with nz == 1.
 struct SumRequest {
     const float4* particles;  // Constraint AoS
     const float* radii;       // nullptr: Phi^ evaluated at |k|
-    float radius_max;         // largest radius if known (registration), else < 0
+    float radius_min;         // smallest / largest radius and largest |weight|
+    float radius_max;         //   when known (registration), else < 0
+    float weight_max;
     int n;
     int basis;
     Lattice lat;
     double scale;
     float2* out;
+    long long out_base, out_sx, out_sy, out_sz;
     int wrap;
     int row;
     bool accumulate;
     cudaStream_t stream;
+    int* error_flag;  // device word set by kernels that give up a bounded wait
 };
 
 // Grow-only device scratch owned by one VisConfig.
@@ -95,9 +100,12 @@ void timer_end(KernelTimer* timer, int stage, cudaStream_t stream);
 
 int device_sm_count();
 
-// Largest radius of a registered group, keyed by its device radii pointer
-// (recorded by vis_register_meshless_dataset); -1 if unknown.
-float registered_radius_max(const float* d_radii);
+// Statistics of a registered group, recorded by vis_register_meshless_dataset
+// and keyed by the group's device particle pointer; all -1 if unknown.
+struct GroupStats {
+    float radius_min = -1.f, radius_max = -1.f, weight_max = -1.f;
+};
+GroupStats registered_group_stats(const void* d_constraints);
 
 // Counts a launch of one of this library's kernels (vis_kernel_launch_count).
 void count_launch();

@@ -267,6 +267,7 @@ struct FinalizeArgs {
     bool factored;
     double scale;
     float2* out;
+    long long out_base, out_sx, out_sy, out_sz;
     int wrap;
     int row;
     bool accumulate;
@@ -298,7 +299,7 @@ __global__ void finalize_kernel(FinalizeArgs f) {
     const float re = (float)(sr * factor), im = (float)(-si * factor);
     size_t idx;
     if (f.wrap > 0) idx = (size_t)(x < 0 ? x + f.wrap : x) * f.row + rest;
-    else idx = (size_t)q;
+    else idx = (size_t)(f.out_base + xi * f.out_sx + (rest / f.lat.nz) * f.out_sy + (rest % f.lat.nz) * f.out_sz);
     if (f.accumulate) {
         float2 o = f.out[idx];
         f.out[idx] = make_float2(o.x + re, o.y + im);
@@ -426,6 +427,10 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     f.factored = factored;
     f.scale = req.scale;
     f.out = req.out;
+    f.out_base = req.out_base;
+    f.out_sx = req.out_sx;
+    f.out_sy = req.out_sy;
+    f.out_sz = req.out_sz;
     f.wrap = req.wrap;
     f.row = req.row;
     f.accumulate = req.accumulate;

@@ -229,3 +229,55 @@ def test_manual_d_image_stream_and_timing():
     cfg.close()
     ref = O.render_direct(groups, (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))
     assert O.rel_l2(img, ref) < SPEC_TOL
+
+
+# ---------------------------------------------------------------- tensor form
+def _tc_groups(rng, n):
+    pos = rng.random((n, 3), dtype=np.float32)
+    w = rng.standard_normal(n).astype(np.float32)
+    h = np.exp(rng.uniform(np.log(0.01), np.log(0.06), n)).astype(np.float32)
+    return {
+        "gauss_decaying_radii": [(constraints(pos, w), h, M.GAUSSIAN_DECAYING)],
+        "sph_no_radii": [(constraints(pos * 0.05, w), None, M.SPH)],
+        "wendland_uniform_radius": [(constraints(pos, w), np.full(n, 0.03, np.float32), M.WENDLAND_D3_C2)],
+        "two_groups": [(constraints(pos[: n // 2], w[: n // 2]), h[: n // 2], M.GAUSSIAN_DECAYING),
+                       (constraints(pos[n // 2:], w[n // 2:]), np.full(n - n // 2, 0.02, np.float32), M.SPH)],
+    }
+
+
+@pytest.mark.parametrize("case", ["gauss_decaying_radii", "sph_no_radii", "wendland_uniform_radius", "two_groups"])
+def test_tensor_form_matches_fp64(case):
+    """Separable groups on a 32x32x17 half-spectrum through the tcgen05 path
+    (FORM_TENSOR), including the Nyquist plane and ragged particle counts."""
+    rng = np.random.default_rng(21)
+    groups = _tc_groups(rng, 3001)[case]
+    grid = (32, 32, 32)
+    spec, imgs = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), rotating_views(3),
+                                    M.FORM_TENSOR)
+    ref = O.spectrum_grid(groups, 1.0, grid)
+    assert O.rel_l2(spec, ref) < SPEC_TOL
+    assert O.rel_l2(spec[:, :, -1], ref[:, :, -1]) < SPEC_TOL  # Nyquist plane (plain form)
+    ref_imgs = O.render_from_spectrum(ref, grid, 1.0, (1.0, 1.0), (16, 16), rotating_views(3), (32, 32))
+    assert O.rel_l2(imgs, ref_imgs) < IMAGE_TOL
+
+
+def test_tensor_form_long_accumulation_random_points():
+    """N = 2^18 decaying-Gaussian particles in 16 h-bins on a 64^3 lattice
+    (8192 particles ... per item, long TMEM accumulation with flushes);
+    FP64 check on 2048 random points, and agreement with the plain form."""
+    rng = np.random.default_rng(22)
+    n = 1 << 18
+    pos = rng.random((n, 3), dtype=np.float32)
+    w = rng.random(n, dtype=np.float32)
+    h = np.exp(rng.uniform(np.log(0.005), np.log(0.05), n)).astype(np.float32)
+    edges = np.exp(np.linspace(np.log(0.005), np.log(0.05), 17))
+    b = np.clip(np.searchsorted(edges, h, side="right") - 1, 0, 15)
+    groups = [(constraints(pos[b == k], w[b == k]), h[b == k], M.GAUSSIAN_DECAYING) for k in range(16)]
+    spec_tc, _ = spectrum_and_views(groups, (64, 64, 64), 1.0, (1.0, 1.0), (32, 32), (64, 64), None, M.FORM_TENSOR)
+    spec_pl, _ = spectrum_and_views(groups, (64, 64, 64), 1.0, (1.0, 1.0), (32, 32), (64, 64), None, M.FORM_PLAIN)
+    prng = np.random.default_rng(3)
+    ijk = np.stack([prng.integers(-32, 32, 2048), prng.integers(-32, 32, 2048), prng.integers(0, 33, 2048)], 1)
+    ref = sum(O.spectrum_points(g[0], g[1], g[2], 1.0, ijk) for g in groups)
+    got = spec_tc[ijk[:, 0] + 32, ijk[:, 1] + 32, ijk[:, 2]]
+    assert O.rel_l2(got, ref) < SPEC_TOL
+    assert O.rel_l2(spec_tc, spec_pl) < SPEC_TOL
