@@ -40,17 +40,88 @@ sys.path.insert(0, str(ROOT))
 FP32_LANES_PER_SM = 128
 
 
+STAGE_NAMES = {0: "plain_sum", 3: "tensor_sum", 1: "slice", 2: "fft"}
+STAGES = tuple(STAGE_NAMES)
+
+
+def sum_terms_split(w):
+    """Terms per step done by the tensor-core kernel if every group takes it
+    (planes l < Kz/2) and by the plain Nyquist plane."""
+    kx, ky, kz = w["grid"]
+    n = sum(len(c) for c, _, _ in w["groups"])
+    return n * kx * ky * (kz // 2), n * kx * ky
+
+
+def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
+    """Roofline of the dominant Fourier-sum kernel: 8 algorithmic flops per
+    particle x frequency term over the kernel's own event-timed duration."""
+    terms, n, g = terms_per_step(w)
+    (p_ms, p_n), (t_ms, t_n) = stage_t[0], stage_t[3]
+    max_mhz = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    if t_ms > p_ms and t_n > 0:
+        tc_terms, _ = sum_terms_split(w)
+        per_launch_terms = tc_terms * steps / t_n
+        launch_s = t_ms / t_n / 1000.0
+        alg = 8.0 * per_launch_terms / launch_s / 1e12
+        issued = 24.0 * per_launch_terms / launch_s / 1e12
+        peak = peaks.get("bf16_tflops", 1590.0)
+        return {"bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak,
+                "traffic": None, "kernel": "tc_sum_kernel", "flops_per_term": 8,
+                "issued_tflops": issued, "issued_frac": issued / peak,
+                "issued_note": "3 FP16 products per term (hi*hi, hi*lo, lo*hi): 24 issued flops per term",
+                "launch_ms": t_ms / t_n, "launches": t_n,
+                "peak_source": f"{peak_src} dense bf16 cuBLAS burst (FP16 dense rate is the same on B200)"}
+    per_launch_terms = terms * steps / max(1, p_n)
+    launch_s = p_ms / max(1, p_n) / 1000.0
+    alg = 8.0 * per_launch_terms / launch_s / 1e12 if launch_s > 0 else 0.0
+    peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    r = {"bound": "fp32", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak, "traffic": None,
+         "kernel": "plain_sum_kernel", "flops_per_term": 8, "launch_ms": p_ms / max(1, p_n), "launches": p_n,
+         "peak_source": f"nominal FP32: {sm_count} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x {max_mhz:.0f} MHz "
+                        "(MEASURED_PEAKS.json has no FP32 figure)"}
+    if clk.get("sm_mhz"):
+        r["frac_at_sampled_clock"] = alg / (peak * clk["sm_mhz"] / max_mhz)
+    return r
+
+
+def compare_forms(M, cfg, sp, ds, w, stream, flush, args, steps=2):
+    """The spectrum sum alone, tensor form vs plain form, same inputs."""
+    import torch
+
+    terms, _, _ = terms_per_step(w)
+    out = {}
+    for name, form in (("tensor", M.FORM_TENSOR), ("plain", M.FORM_PLAIN)):
+        sp.compute(cfg, ds, form)
+        cfg.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.zero_()
+                ev[k][0].record(stream)
+                sp.compute(cfg, ds, form)
+                ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        out[name] = {"ms_per_sum": ms, "gterms_per_s": terms / (ms / 1000.0) / 1e9}
+    out["ratio"] = out["tensor"]["gterms_per_s"] / out["plain"]["gterms_per_s"]
+    out["workload"] = w["name"]
+    return out
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3"], default="c2",
-                   help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views (profiling case)")
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s"], default="c2",
+                   help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
+                        "N=2^17, 128^3, 4 h-bins (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--compare-forms", action="store_true",
+                   help="also time the spectrum sum alone in the tensor and the plain form (tc_vs_plain)")
     return p.parse_args()
 
 
@@ -61,6 +132,10 @@ def workload(name):
         return W.c1()
     if name == "c3":
         return W.c3()
+    if name == "c3s":
+        w = W.c3(n=1 << 17, grid=128, bins=4)
+        w["name"] = "C3-small"
+        return w
     if name == "c2s":
         w = W.c2(n=65536, grid=64, views=16)
         w["name"] = "C2-small"
@@ -255,7 +330,7 @@ def run_ours(args):
         step()
     cfg.synchronize()
     cfg.enable_timing(True)
-    for st in (M.STAGE_SUM, M.STAGE_SLICE, M.STAGE_FFT):
+    for st in STAGES:
         cfg.kernel_time(st)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     clocks = Clocks(torch.cuda.current_device())
@@ -274,31 +349,19 @@ def run_ours(args):
     launches = lib.vis_kernel_launch_count() - launches0
     clk = clocks.stop()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
-    sum_ms, sum_n = cfg.kernel_time(M.STAGE_SUM)
-    sl_ms, sl_n = cfg.kernel_time(M.STAGE_SLICE)
-    fft_ms, fft_n = cfg.kernel_time(M.STAGE_FFT)
+    stage_t = {st: cfg.kernel_time(st) for st in STAGES}
     cfg.enable_timing(False)
     t_max = allmax(t_ms)
     sec = t_max / 1000.0
     value = world * terms * args.steps / sec / 1e9
     views_per_s = world * nv * args.steps / sec
 
-    # dominant kernel: the Fourier-sum kernel(s)
     peaks, peak_src = measured_peaks()
-    sum_launch_ms = sum_ms / max(1, sum_n)
-    terms_per_launch = terms * args.steps / max(1, sum_n)
-    achieved_tflops = 8.0 * terms_per_launch / (sum_launch_ms / 1000.0) / 1e12
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
-    max_mhz = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
-    roofline = {"bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved_tflops / fp32_peak, "traffic": None,
-                "kernel": "plain_sum_kernel", "flops_per_term": 8,
-                "peak_source": f"nominal FP32: {sm_count} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x {max_mhz:.0f} MHz "
-                               "(MEASURED_PEAKS.json has no FP32 figure)"}
-    if clk.get("sm_mhz"):
-        roofline["frac_at_sampled_clock"] = achieved_tflops / (fp32_peak * clk["sm_mhz"] / max_mhz)
-
+    roofline = sum_roofline(stage_t, w, args.steps, peaks, peak_src, clk, sm_count)
+    comparison = None
+    if args.compare_forms:
+        comparison = compare_forms(M, cfg, sp, ds, w, stream, flush, args)
     # end to end through the public C API with host buffers
     e2e = None
     if not args.no_e2e:
@@ -366,14 +429,15 @@ def run_ours(args):
                            "l2": "flushed between timed steps (256 MB write outside the event pair)",
                            "parallelism": f"replicas x{world}"},
                 "views_per_s": views_per_s,
-                "stages_ms_per_step": {"sum": sum_ms / args.steps, "slice": sl_ms / args.steps,
-                                       "fft": fft_ms / args.steps},
+                "stages_ms_per_step": {name: stage_t[st][0] / args.steps for st, name in STAGE_NAMES.items()},
                 "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),
                 "peaks_source": peak_src}
         if e2e:
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if comparison:
+            line["tc_vs_plain"] = comparison
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

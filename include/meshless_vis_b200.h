@@ -99,9 +99,10 @@ int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int 
 /* ----------------------------------------------------------------- timing */
 enum VisTimingStage
 {
-    VIS_STAGE_SUM = 0,   /* Fourier-sum kernels (direct slice and 3D spectrum) */
-    VIS_STAGE_SLICE = 1, /* slice extraction into the C2R layout */
-    VIS_STAGE_FFT = 2    /* cuFFT C2R */
+    VIS_STAGE_SUM = 0,        /* plain-form Fourier-sum kernels (direct slice and 3D spectrum) */
+    VIS_STAGE_SLICE = 1,      /* slice extraction into the C2R layout */
+    VIS_STAGE_FFT = 2,        /* cuFFT C2R */
+    VIS_STAGE_TENSOR_SUM = 3  /* tensor-core Fourier-sum kernels */
 };
 /* When enabled, CUDA events bracket every launch of each stage on the
  * config's stream.  vis_config_kernel_timing waits for them, returns the summed

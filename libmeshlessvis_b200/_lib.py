@@ -37,7 +37,7 @@ BASIS_NAMES = {"sph": SPH, "gaussian": GAUSSIAN, "wendland_d3_c2": WENDLAND_D3_C
 
 # include/meshless_vis_b200.h: enum VisSumForm / VisTimingStage / VisError
 FORM_AUTO, FORM_PLAIN, FORM_TENSOR = 0, 1, 2
-STAGE_SUM, STAGE_SLICE, STAGE_FFT = 0, 1, 2
+STAGE_SUM, STAGE_SLICE, STAGE_FFT, STAGE_TENSOR_SUM = 0, 1, 2, 3
 VIS_SUCCESS = 0
 
 # Constraint: __align__(16) { float3 position; float weight; }

@@ -115,8 +115,9 @@ void Workspace::release() {
 // ------------------------------------------------------------------ timing
 struct KernelTimer {
     bool enabled = false;
-    cudaEvent_t open[3] = {nullptr, nullptr, nullptr};
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> done[3];
+    static constexpr int kStagesTimed = 4;
+    cudaEvent_t open[kStagesTimed] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> done[kStagesTimed];
     std::vector<cudaEvent_t> pool;
 
     cudaEvent_t take() {
@@ -137,7 +138,7 @@ struct KernelTimer {
         done[s].clear();
     }
     ~KernelTimer() {
-        for (int s = 0; s < 3; ++s) {
+        for (int s = 0; s < kStagesTimed; ++s) {
             clear_stage(s);
             if (open[s]) pool.push_back(open[s]);
         }
@@ -644,7 +645,8 @@ int vis_config_enable_kernel_timing(VisConfig* c, int enable) {
 
 int vis_config_kernel_timing(VisConfig* c, int stage, float* total_ms, int* launches) {
     ConfigState* s = c ? state_of(c) : nullptr;
-    if (!s || stage < 0 || stage > 2) return set_error(kInvalidValue, "vis_config_kernel_timing: bad arguments");
+    if (!s || stage < 0 || stage >= KernelTimer::kStagesTimed)
+        return set_error(kInvalidValue, "vis_config_kernel_timing: bad arguments");
     float total = 0.f;
     int count = 0;
     for (auto& p : s->timer.done[stage]) {

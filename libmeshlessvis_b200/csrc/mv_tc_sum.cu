@@ -614,10 +614,10 @@ int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, Kern
         st = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes),
                         "cudaFuncSetAttribute");
         if (st != kOk) return st;
-        timer_begin(timer, 0, req.stream);
+        timer_begin(timer, 3, req.stream);
         kern<<<(unsigned)(ftiles * splits), kThreads, kSmemBytes, req.stream>>>(a);
         count_launch();
-        timer_end(timer, 0, req.stream);
+        timer_end(timer, 3, req.stream);
         st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");
         if (st != kOk) return st;
     }

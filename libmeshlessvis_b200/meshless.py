@@ -12,14 +12,14 @@ import numpy as np
 
 from . import _lib as L
 from ._lib import (CONSTRAINT_DTYPE, FORM_AUTO, FORM_PLAIN, FORM_TENSOR, GAUSSIAN, GAUSSIAN_DECAYING, SPH,
-                   STAGE_FFT, STAGE_SLICE, STAGE_SUM, WENDLAND_D3_C2, Group, MeshlessDataset, VisError, float2,
+                   STAGE_FFT, STAGE_SLICE, STAGE_SUM, STAGE_TENSOR_SUM, WENDLAND_D3_C2, Group, MeshlessDataset, VisError, float2,
                    float3, int2, int3)
 
 __all__ = ["get_simple_meshless_dataset", "delete_meshless_dataset", "delete_meshless_datasets",
            "get_number_of_terms", "load_meshless_datasets_from_file", "save_meshless_datasets_to_file",
            "shift_meshless_dataset", "Dataset", "Config", "Spectrum", "constraints_from_arrays", "VisError",
            "SPH", "GAUSSIAN", "WENDLAND_D3_C2", "GAUSSIAN_DECAYING", "FORM_AUTO", "FORM_PLAIN", "FORM_TENSOR",
-           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT"]
+           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT", "STAGE_TENSOR_SUM"]
 
 
 def lib():
