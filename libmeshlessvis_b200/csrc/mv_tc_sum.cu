@@ -17,35 +17,46 @@
 // Real embedding with re/im interleaved along K (k = 2j + {0,1}):
 //   A'[m, 2j..2j+1] = (Re A, Im A),  B'_re[2j..2j+1, n] = (Re B, -Im B),
 //   B'_im[2j..2j+1, n] = (Im B, Re B);  C = A' [B'_re | B'_im] = [Re F | Im F].
-// Split precision: every operand is x = hi + lo / 2048 with hi, lo FP16;
-//   D_main = A_hi B_hi,  D_corr = A_hi B_lo + A_lo B_hi,  C = D_main + D_corr / 2048
-// (product error ~2^-22 relative).  Accumulators live in TMEM (FP32); every
-// kFlushStages stages the flush warps fold them into a Kahan-compensated FP32
-// running total also kept in TMEM (bounding the length of any tensor-core
-// accumulation chain), and at the end of the particle range add the total to
-// an FP64 accumulator in global memory (one RED.ADD.F64 per frequency and
-// item).  A finalize kernel converts to the float2 spectrum.
+// Split precision: operands are scaled by 2^12 (exact) and split as
+// x 2^12 = hi + lo with hi, lo FP16; the scale keeps lo a normal FP16 number
+// for every |x| >= 2^-15 (below that the absolute error is < 2^-36).  The three
+// products hi*hi + hi*lo + lo*hi (error ~2^-22 relative) accumulate into ONE
+// TMEM accumulator (FP32, units of 2^24).  Two accumulators alternate: while the
+// MMAs fill one, the flush warps fold the other into a Kahan-compensated FP32
+// running total also kept in TMEM.  This bounds every tensor-core accumulation
+// chain to flush_stages x 12 MMAs (the tensor core's FP32 accumulation loses
+// accuracy with chain length: 1.2e-6 rel-L2 at 4 stages, 5.2e-6 at 64).  At
+// the end of the particle range the total is added to an FP64 accumulator in
+// global memory (one RED.ADD.F64 per frequency and work item), which a
+// finalize kernel converts to the float2 spectrum.
 //
 // CTA tile: M = 128 rows (a, b) (8-row chunks of constant a), N = 64 c values
 // (128 real columns), K = 32 particles (64 real) per pipeline stage, 3 stages.
-// Warp roles: warp 0 allocates TMEM and issues tcgen05.mma (one thread);
-// warps 1-4 flush TMEM (warp w reads lanes 32 (w % 4) .. +31); warps 5-12
-// generate operands straight into shared memory in the canonical no-swizzle
-// K-major layout (8x16-byte core matrices; 16 bytes of padding between K
-// columns of core matrices keep the producer stores free of bank conflicts).
-// Operands are produced by recurrences along b and c (8 steps from an exact
-// fixed-point start, moving away from the axis origin so that Gaussian factors
-// only shrink along a chain).
+// Warp roles:
+//   warp 0       allocates TMEM, one thread issues tcgen05.mma / commit;
+//   warps 1-4    flush TMEM (warp w reads lanes 32 (w % 4) .. +31);
+//   warps 5-16   generate operands straight into shared memory in the
+//                canonical no-swizzle K-major layout (8x16-byte core matrices;
+//                16 bytes of padding between K columns of core matrices keep
+//                the stores free of bank conflicts), by recurrences along b and
+//                c (8 steps from an exact fixed-point start, moving away from
+//                the axis origin so Gaussian factors only shrink along a chain);
+//   warp 17      streams the per-particle constants of each stage into shared
+//                memory with cp.async.bulk (global -> own CTA, no multicast),
+//                three stages ahead.
+// Per-particle constants (fixed-point positions, unit rotations, Gaussian
+// ratios) are computed once per launch by tc_prep_kernel.
 //
 // Every mbarrier wait is bounded (2 s of %globaltimer); a wait that runs out
 // sets *error_flag, raises the CTA's abort flag, and all roles leave their
 // loops; warp 0 drains its MMAs (bounded) before releasing TMEM.  The host
-// reports a non-zero flag at the next synchronising call.  No TMA, no
-// clusters, no multicast.
+// reports a non-zero flag at the next synchronising call.  No TMA tensor maps,
+// no clusters, no multicast.
 #include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "mv_device.cuh"
 #include "mv_internal.h"
@@ -60,35 +71,48 @@ constexpr int kN = 2 * kNc;
 constexpr int kKp = 32;
 constexpr int kKr = 2 * kKp;
 constexpr int kStages = 3;
-constexpr int kFlushStages = 4;  // 4 stages x 4 MMA K-steps: 16 accumulations per chain
 constexpr int kCoreBytes = 128;
 constexpr int kLbo = 16 * kCoreBytes + 16;          // bytes between K-adjacent core matrices
 constexpr int kOperandBytes = (kKr / 8) * kLbo;     // 8 K-columns of 16 core matrices
 constexpr int kStageBytes = 4 * kOperandBytes;      // A_hi, A_lo, B_hi, B_lo
-constexpr int kProducerWarps = 8;
+constexpr int kParticleBytes = 48;                  // sizeof(TcParticle)
+constexpr int kSlotBytes = kKp * kParticleBytes;    // particle constants of one stage
+constexpr int kProducerWarps = 12;  // 8 warps of A units + 4 warps of B units, 2 chains each
 constexpr int kFlushWarps = 4;
-constexpr int kThreads = 32 * (1 + kFlushWarps + kProducerWarps);
+constexpr int kLoaderWarp = 1 + kFlushWarps + kProducerWarps;
+constexpr int kThreads = 32 * (kLoaderWarp + 1);
 constexpr int kProducerThreads = 32 * kProducerWarps;
 constexpr int kFlushThreads = 32 * kFlushWarps;
-constexpr uint32_t kTmemCols = 512;  // main | corr | total | compensation, 128 columns each
-constexpr float kLoScale = 2048.f;
-constexpr float kInvLoScale = 1.f / 2048.f;
+constexpr uint32_t kTmemCols = 512;  // accumulator 0 | accumulator 1 | total | compensation
+constexpr uint32_t kColTotal = 2 * kN, kColComp = 3 * kN;
+constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
+constexpr float kInvProductScale = 1.f / (4096.f * 4096.f);  // 2^-24
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
-constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 256;
+constexpr size_t kBarrierOffset = (size_t)kStages * (kStageBytes + kSlotBytes);
+constexpr size_t kSmemBytes = kBarrierOffset + 256;
 
 // idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, N = 128, M = 128.
 constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
 
+// Per-particle constants of one group, computed once per launch by
+// tc_prep_kernel (48 bytes, three float4 loads).
+struct __align__(16) TcParticle {
+    uint32_t qx, qy, qz;  // fixed-point turns of step * position
+    float amp;            // 2^12 w / W
+    float gam;            // -pi log2(e) step^2 h^2 (GAUSSIAN_DECAYING), else 0
+    float rho2;           // exp2(2 gam): ratio of successive Gaussian step factors
+    float2 ry, rz;        // exp(-2 pi i Qy / 2^32), exp(-2 pi i Qz / 2^32), accurate
+    float pad[2];
+};
+static_assert(sizeof(TcParticle) == kParticleBytes, "TcParticle layout");
+
 struct TcArgs {
-    const float4* particles;
-    const float* radii;
+    const TcParticle* tp;
     int k_begin, k_end;  // particle range of the group
     int kx, ky, lz_tc;   // lattice extents; c planes [0, lz_tc) are summed here
     int n_mtiles, n_ntiles;
     int k_chunk;  // particles per work item (multiple of kKp)
-    double step;
-    float gamma_scale;  // -pi log2(e) step^2 (GAUSSIAN_DECAYING), 0 otherwise
-    float inv_wmax;
+    int flush_stages;  // stages per TMEM accumulation chain (4 MMA K-steps each)
     double wmax;
     double* acc;  // [(a_idx * ky + b_idx) * lz_tc + c][2]
     int* error_flag;
@@ -139,6 +163,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// Plain bulk copy global -> this CTA's shared memory, completing on an mbarrier.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -165,28 +202,24 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-    uint32_t r[32];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
         "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
-        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]),
-        "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]),
-        "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
         : "memory");
 }
 
@@ -210,12 +243,13 @@ __device__ __forceinline__ float2 unit_phase(uint32_t q) {
     return make_float2(c, -s);
 }
 
+// Two complex values (already scaled by 2^12) -> FP16 hi and lo pairs.
 __device__ __forceinline__ uint2 pack_hi_lo(float2 z0, float2 z1, uint2* lo_out) {
     const __half2 h0 = __floats2half2_rn(z0.x, z0.y);
     const __half2 h1 = __floats2half2_rn(z1.x, z1.y);
     const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
-    const __half2 l0 = __floats2half2_rn((z0.x - f0.x) * kLoScale, (z0.y - f0.y) * kLoScale);
-    const __half2 l1 = __floats2half2_rn((z1.x - f1.x) * kLoScale, (z1.y - f1.y) * kLoScale);
+    const __half2 l0 = __floats2half2_rn(z0.x - f0.x, z0.y - f0.y);
+    const __half2 l1 = __floats2half2_rn(z1.x - f1.x, z1.y - f1.y);
     lo_out->x = *reinterpret_cast<const uint32_t*>(&l0);
     lo_out->y = *reinterpret_cast<const uint32_t*>(&l1);
     return make_uint2(*reinterpret_cast<const uint32_t*>(&h0), *reinterpret_cast<const uint32_t*>(&h1));
@@ -230,14 +264,16 @@ __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_secon
 template <bool GAUSS>
 __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    uint64_t* full = bars;                 // [kStages]
-    uint64_t* empty = bars + kStages;      // [kStages]
-    uint64_t* acc_full = bars + 2 * kStages;
-    uint64_t* acc_empty = acc_full + 1;
-    uint64_t* drain = acc_full + 2;
-    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(acc_full + 3);
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(acc_full + 3) + 1;
+    uint8_t* slots = smem + kStages * kStageBytes;  // [kStages][kSlotBytes]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBarrierOffset);
+    uint64_t* full = bars;                   // [kStages] producers -> MMA
+    uint64_t* empty = bars + kStages;        // [kStages] MMA -> producers
+    uint64_t* pdata = bars + 2 * kStages;    // [kStages] loader -> producers
+    uint64_t* acc_full = bars + 3 * kStages;   // [2] MMA -> flush
+    uint64_t* acc_empty = acc_full + 2;         // [2] flush -> MMA
+    uint64_t* drain = acc_full + 4;
+    volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(acc_full + 5);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(acc_full + 5) + 1;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -251,15 +287,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     const int kb = a.k_begin + ks * a.k_chunk;
     const int ke = min(a.k_end, kb + a.k_chunk);
     const int n_stages = max(0, (ke - kb + kKp - 1) / kKp);
-    const int n_chunks = (n_stages + kFlushStages - 1) / kFlushStages;
+    const int flush_stages = a.flush_stages;
+    const int n_chunks = (n_stages + flush_stages - 1) / flush_stages;
 
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
             mbar_init(&full[i], kProducerThreads);
             mbar_init(&empty[i], 1);
+            mbar_init(&pdata[i], 1);
         }
-        mbar_init(acc_full, 1);
-        mbar_init(acc_empty, kFlushThreads);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], kFlushThreads);
+        }
         mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -281,24 +321,26 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         if (lane == 0) {
             for (int s = 0; s < n_stages; ++s) {
                 const int buf = s % kStages;
-                const int k = s / kFlushStages;
-                const bool first = (s % kFlushStages) == 0;
-                if (first && k > 0 && !mbar_wait(acc_empty, (k - 1) & 1, abort_flag, a.error_flag, 1)) break;
+                const int k = s / flush_stages;
+                const int b = k & 1;
+                const bool first = (s % flush_stages) == 0;
+                if (first && k >= 2 && !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1, abort_flag, a.error_flag, 1))
+                    break;
                 if (!mbar_wait(&full[buf], (s / kStages) & 1, abort_flag, a.error_flag, 2)) break;
                 tc_fence_after();
                 const uint32_t base = smem_u32(smem + buf * kStageBytes);
                 const uint32_t a_hi = base, a_lo = base + kOperandBytes;
                 const uint32_t b_hi = base + 2 * kOperandBytes, b_lo = base + 3 * kOperandBytes;
+                const uint32_t d = tmem + (uint32_t)(b * kN);
 #pragma unroll
                 for (int t = 0; t < kKr / 16; ++t) {
                     const uint32_t off = (uint32_t)(2 * t * kLbo);
-                    const uint32_t acc = (first && t == 0) ? 0u : 1u;
-                    mma_f16(tmem + 0, smem_desc(a_hi + off), smem_desc(b_hi + off), acc);
-                    mma_f16(tmem + kN, smem_desc(a_hi + off), smem_desc(b_lo + off), acc);
-                    mma_f16(tmem + kN, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
+                    mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), (first && t == 0) ? 0u : 1u);
+                    mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), 1u);
+                    mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
                 }
                 mma_commit(&empty[buf]);
-                if ((s % kFlushStages) == kFlushStages - 1 || s == n_stages - 1) mma_commit(acc_full);
+                if ((s % flush_stages) == flush_stages - 1 || s == n_stages - 1) mma_commit(&acc_full[b]);
             }
             mma_commit(drain);
         }
@@ -309,22 +351,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;  // M row owned by this thread
         for (int k = 0; k < n_chunks; ++k) {
-            if (!mbar_wait(acc_full, k & 1, abort_flag, a.error_flag, 4)) break;
+            const int b = k & 1;
+            if (!mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4)) break;
             tc_fence_after();
             const bool last = k == n_chunks - 1;
 #pragma unroll 1
-            for (int cc = 0; cc < kN / 32; ++cc) {
-                float mn[32], cr[32], tt[32], cp[32];
-                tmem_ld32(lane_base + cc * 32, mn);
-                tmem_ld32(lane_base + kN + cc * 32, cr);
+            for (int cc = 0; cc < kN / 16; ++cc) {
+                float dv[16], tt[16], cp[16];
+                tmem_ld16(lane_base + b * kN + cc * 16, dv);
                 if (k > 0) {
-                    tmem_ld32(lane_base + 2 * kN + cc * 32, tt);
-                    tmem_ld32(lane_base + 3 * kN + cc * 32, cp);
+                    tmem_ld16(lane_base + kColTotal + cc * 16, tt);
+                    tmem_ld16(lane_base + kColComp + cc * 16, cp);
                 }
                 tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const float v = fmaf(cr[i], kInvLoScale, mn[i]);
+                for (int i = 0; i < 16; ++i) {
+                    const float v = dv[i] * kInvProductScale;
                     if (k == 0) {
                         tt[i] = v;
                         cp[i] = 0.f;
@@ -336,15 +378,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     }
                 }
                 if (!last) {
-                    tmem_st32(lane_base + 2 * kN + cc * 32, tt);
-                    tmem_st32(lane_base + 3 * kN + cc * 32, cp);
+                    tmem_st16(lane_base + kColTotal + cc * 16, tt);
+                    tmem_st16(lane_base + kColComp + cc * 16, cp);
                 } else {
                     // add the item's total to the FP64 accumulator
                     const int rho = m_tile * kM + row;
                     const int c0 = n_tile * kNc;
-#pragma unroll 4
-                    for (int i = 0; i < 32; ++i) {
-                        const int n = cc * 32 + i;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int n = cc * 16 + i;
                         const int c = c0 + (n % kNc);
                         if (c < a.lz_tc) {
                             const double v = ((double)tt[i] - (double)cp[i]) * a.wmax;
@@ -355,65 +397,84 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             }
             tmem_wait_st();
             tc_fence_before();
-            mbar_arrive(acc_empty);
+            mbar_arrive(&acc_empty[b]);
         }
+    } else if (warp == kLoaderWarp) {
+        // ---------------------------------------------------------- loader
+        if (lane == 0) {
+            for (int s = 0; s < n_stages; ++s) {
+                const int buf = s % kStages;
+                // the producers are done with this slot once stage s - kStages is full
+                if (s >= kStages && !mbar_wait(&full[buf], ((s / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
+                    break;
+                const int j0 = kb + s * kKp;
+                const uint32_t bytes = (uint32_t)(min(kKp, ke - j0) * kParticleBytes);
+                mbar_arrive_expect_tx(&pdata[buf], bytes);
+                bulk_copy_g2s(slots + buf * kSlotBytes, a.tp + j0, bytes, &pdata[buf]);
+            }
+        }
+        __syncwarp();
     } else {
         // -------------------------------------------------------- producers
         const int p = tid - 32 * (1 + kFlushWarps);
         const int pp = p & 15;  // particle pair within the stage
-        // A unit: 8-row chunk rc of the M tile
-        const int rc = p >> 4;
+        // A unit (p < 256): 8-row chunk rc of the M tile
+        const bool has_a = p < 256;
+        const int rc = (p >> 4) & 15;
         const int rho0 = m_tile * kM + rc * 8;
         const int a_x = rho0 / a.ky - a.kx / 2;
         const int b0 = rho0 % a.ky - a.ky / 2;
         const bool a_up = b0 >= 0;
         const int b_s = a_up ? b0 : b0 + 7;
-        // B unit (p < 128): 8-column chunk cb of the N tile
-        const bool has_b = p < 128;
+        // B unit (p >= 256): 8-column chunk cb of the N tile
         const int cb = (p >> 4) & 7;
         const int c_s = n_tile * kNc + cb * 8;
 
         for (int s = 0; s < n_stages; ++s) {
             const int buf = s % kStages;
-            if (!mbar_wait(&empty[buf], ((s / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)) break;
-            uint8_t* st = smem + buf * kStageBytes;
-            uint32_t Qx[2], Qy[2], Qz[2];
-            float amp[2], gam[2];
+            if (!mbar_wait(&pdata[buf], (s / kStages) & 1, abort_flag, a.error_flag, 64)) break;
+            uint32_t pqx[2], pqy[2], pqz[2];
+            float pamp[2], pgam[2], prho2[2];
+            float2 pry[2], prz[2];
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
-                const int j = kb + s * kKp + 2 * pp + e;
-                if (j < ke) {
-                    const float4 q = __ldg(a.particles + j);
-                    Qx[e] = fixed_turns(a.step * (double)q.x);
-                    Qy[e] = fixed_turns(a.step * (double)q.y);
-                    Qz[e] = fixed_turns(a.step * (double)q.z);
-                    amp[e] = q.w * a.inv_wmax;
-                    if constexpr (GAUSS) {
-                        const float h = __ldg(a.radii + j);
-                        gam[e] = a.gamma_scale * h * h;
-                    } else {
-                        gam[e] = 0.f;
-                    }
+                const int jj = 2 * pp + e;
+                if (kb + s * kKp + jj < ke) {
+                    const float4* src = reinterpret_cast<const float4*>(slots + buf * kSlotBytes + jj * kParticleBytes);
+                    const float4 v0 = src[0], v1 = src[1], v2 = src[2];
+                    pqx[e] = __float_as_uint(v0.x);
+                    pqy[e] = __float_as_uint(v0.y);
+                    pqz[e] = __float_as_uint(v0.z);
+                    pamp[e] = v0.w;
+                    pgam[e] = v1.x;
+                    prho2[e] = v1.y;
+                    pry[e] = make_float2(v1.z, v1.w);
+                    prz[e] = make_float2(v2.x, v2.y);
                 } else {
-                    Qx[e] = Qy[e] = Qz[e] = 0u;
-                    amp[e] = 0.f;
-                    gam[e] = 0.f;
+                    pqx[e] = pqy[e] = pqz[e] = 0u;
+                    pamp[e] = 0.f;
+                    pgam[e] = 0.f;
+                    prho2[e] = 1.f;
+                    pry[e] = prz[e] = make_float2(1.f, 0.f);
                 }
             }
-            // ---- A: rows rc*8 .. rc*8+7, particles 2pp, 2pp+1
-            {
-                float2 z[2], R[2];
-                float q[2], rq[2];
+            if (!mbar_wait(&empty[buf], ((s / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)) break;
+            uint8_t* st = smem + buf * kStageBytes;
+            float2 z[2], R[2];
+            float q[2], rq[2];
+            if (has_a) {
+                // ---- A: rows rc*8 .. rc*8+7, particles 2pp, 2pp+1 (amp includes 2^12)
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const float2 u = unit_phase((uint32_t)a_x * Qx[e] + (uint32_t)b_s * Qy[e]);
-                    float g = amp[e];
-                    if constexpr (GAUSS) g *= exp2f(gam[e] * (float)(a_x * a_x + b_s * b_s));
-                    z[e] = make_float2(g * u.x, g * u.y);
-                    R[e] = unit_phase(a_up ? Qy[e] : (uint32_t)(0u - Qy[e]));
+                    float sn, cs;
+                    __sincosf(turns_to_radians((uint32_t)a_x * pqx[e] + (uint32_t)b_s * pqy[e]), &sn, &cs);
+                    float g = pamp[e];
+                    if constexpr (GAUSS) g *= exp2f(pgam[e] * (float)(a_x * a_x + b_s * b_s));
+                    z[e] = make_float2(g * cs, -g * sn);
+                    R[e] = a_up ? pry[e] : make_float2(pry[e].x, -pry[e].y);
                     if constexpr (GAUSS) {
-                        q[e] = exp2f(gam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
-                        rq[e] = exp2f(2.f * gam[e]);
+                        q[e] = exp2f(pgam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
+                        rq[e] = prho2[e];
                     } else {
                         q[e] = 1.f;
                         rq[e] = 1.f;
@@ -438,22 +499,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         if constexpr (GAUSS) q[e] *= rq[e];
                     }
                 }
-            }
-            // ---- B: columns cb*8 .. cb*8+7 (Re) and 64 + ... (Im)
-            if (has_b) {
-                float2 z[2], R[2];
-                float q[2], rq[2];
+            } else {
+                // ---- B: columns cb*8 .. cb*8+7 (Re) and 64 + ... (Im), scaled by 2^12
                 const bool live = c_s < a.lz_tc;
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const float2 u = unit_phase((uint32_t)c_s * Qz[e]);
-                    float g = live ? 1.f : 0.f;
-                    if constexpr (GAUSS) g *= exp2f(gam[e] * (float)(c_s * c_s));
-                    z[e] = make_float2(g * u.x, g * u.y);
-                    R[e] = unit_phase(Qz[e]);
+                    float sn, cs;
+                    __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
+                    float g = live ? kOperandScale : 0.f;
+                    if constexpr (GAUSS) g *= exp2f(pgam[e] * (float)(c_s * c_s));
+                    z[e] = make_float2(g * cs, -g * sn);
+                    R[e] = prz[e];
                     if constexpr (GAUSS) {
-                        q[e] = exp2f(gam[e] * (float)(2 * c_s + 1));
-                        rq[e] = exp2f(2.f * gam[e]);
+                        q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
+                        rq[e] = prho2[e];
                     } else {
                         q[e] = 1.f;
                         rq[e] = 1.f;
@@ -512,6 +571,39 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     }
 }
 
+struct TcPrepArgs {
+    const float4* particles;
+    const float* radii;
+    int n;
+    double step;
+    float gamma_scale;
+    float inv_wmax;
+    bool gauss;
+    TcParticle* out;
+};
+
+__global__ void tc_prep_kernel(TcPrepArgs p) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.n) return;
+    const float4 q = p.particles[j];
+    TcParticle t;
+    t.qx = fixed_turns(p.step * (double)q.x);
+    t.qy = fixed_turns(p.step * (double)q.y);
+    t.qz = fixed_turns(p.step * (double)q.z);
+    t.amp = q.w * p.inv_wmax * kOperandScale;
+    if (p.gauss) {
+        const float h = p.radii[j];
+        t.gam = p.gamma_scale * h * h;
+    } else {
+        t.gam = 0.f;
+    }
+    t.rho2 = exp2f(2.f * t.gam);
+    t.ry = unit_phase(t.qy);
+    t.rz = unit_phase(t.qz);
+    t.pad[0] = t.pad[1] = 0.f;
+    p.out[j] = t;
+}
+
 // acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
 // Phi^ factor (groups whose Phi^ factors out) and the scale, written or added.
 struct TcFinalizeArgs {
@@ -558,6 +650,17 @@ bool is_spectrum_lattice(const Lattice& L) {
            L.m[6] == 0 && L.m[7] == 0;
 }
 
+// Stages per TMEM accumulation chain before the flush into the compensated
+// total: MV_TC_FLUSH_STAGES (1..1024) overrides the default.
+int tc_flush_stages() {
+    static const int v = [] {
+        const char* e = std::getenv("MV_TC_FLUSH_STAGES");
+        const int x = e ? std::atoi(e) : 0;
+        return (x >= 1 && x <= 1024) ? x : 8;
+    }();
+    return v;
+}
+
 }  // namespace
 
 int tensor_sum_available(const SumRequest& r) {
@@ -585,9 +688,24 @@ int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, Kern
     if (st != kOk) return st;
 
     if (req.n > 0 && req.weight_max > 0.f) {
+        st = ws.reserve((size_t)req.n * sizeof(TcParticle));
+        if (st != kOk) return st;
+        TcPrepArgs pa;
+        pa.particles = req.particles;
+        pa.radii = req.radii;
+        pa.n = req.n;
+        pa.step = L.kx;
+        pa.gamma_scale = gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
+        pa.inv_wmax = 1.0f / req.weight_max;
+        pa.gauss = gauss;
+        pa.out = static_cast<TcParticle*>(ws.ptr);
+        tc_prep_kernel<<<(req.n + 255) / 256, 256, 0, req.stream>>>(pa);
+        count_launch();
+        st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
+        if (st != kOk) return st;
+
         TcArgs a;
-        a.particles = req.particles;
-        a.radii = req.radii;
+        a.tp = pa.out;
         a.k_begin = 0;
         a.k_end = req.n;
         a.kx = kx;
@@ -604,9 +722,7 @@ int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, Kern
         splits = (req.n + chunk - 1) / chunk;
         if (ftiles * splits > (1LL << 31) - 1) return set_error(kInvalidValue, "tensor sum: too many work items");
         a.k_chunk = (int)chunk;
-        a.step = L.kx;
-        a.gamma_scale = gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
-        a.inv_wmax = 1.0f / req.weight_max;
+        a.flush_stages = tc_flush_stages();
         a.wmax = req.weight_max;
         a.acc = static_cast<double*>(acc.ptr);
         a.error_flag = req.error_flag;
