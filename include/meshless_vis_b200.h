@@ -115,6 +115,36 @@ int vis_config_kernel_timing(VisConfig* vis_config, int stage, float* total_ms, 
  * (cuFFT's kernels are not counted). */
 unsigned long long vis_kernel_launch_count(void);
 
+/* ------------------------------------------------------- no allocation */
+/* This entry point has no counterpart in the reference.  It is for callers
+ * that cannot allocate device memory: code that must keep a fixed device
+ * footprint, renders inside a frame loop where a cudaMalloc (and the
+ * device-wide synchronisation that a cudaFree brings) is not acceptable, or
+ * lives under another framework's memory pool.
+ *
+ * It does, for one group, the direct slice sum of vis_fourier_volume_rendering
+ * (sample_fourier_transform_over_grid plus arrange_samples): writes (or, with
+ * accumulate != 0, adds) step.x*step.y * sum_j w_j Phi^(r h_j)
+ * exp(-2 pi i f.x_j) at every slice sample into d_arranged, the C2R layout
+ * float2[number_of_samples.x][number_of_samples.y/2 + 1].  Elements that are
+ * not slice samples are left untouched: zero the buffer once.  All buffers are
+ * the caller's device memory (d_radii may be NULL: Phi^ at r itself).  Work is
+ * enqueued on `stream`; the call does not wait.
+ *
+ * It allocates nothing.  Its scratch (split-K partial sums and the Phi^ table)
+ * is a fixed 8 MiB array in the library's device image, which every GPU that
+ * loads the library holds until the process exits; slices of more than about
+ * 1.04 million samples are rejected with VIS_ERROR_INVALID_VALUE.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  All calls share the one
+ * array: calls whose work overlaps on the GPU (different streams, or different
+ * host threads on one device) race and must be serialised by the caller.
+ * Returns VIS_SUCCESS or a VisError code. */
+int vis_fourier_slice_sum_noalloc(const Constraint* d_constraints, const float* d_radii, int number_of_terms,
+                                  BasisFunctionId basis_function_id, float2 step_size, int2 cutoff_frequency,
+                                  float3 u_axis, float3 v_axis, int2 number_of_samples, float2* d_arranged,
+                                  int accumulate, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,8 @@ SIGNATURES = {
     "vis_config_enable_kernel_timing": (c_int, [PConfig, c_int]),
     "vis_config_kernel_timing": (c_int, [PConfig, c_int, POINTER(c_float), POINTER(c_int)]),
     "vis_kernel_launch_count": (ctypes.c_ulonglong, []),
+    "vis_fourier_slice_sum_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, float2, int2, float3, float3, int2,
+                                              c_void_p, c_int, c_void_p]),
 }
 
 _lib = None

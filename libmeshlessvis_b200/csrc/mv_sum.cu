@@ -34,7 +34,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
 
+#include "meshless.h"
 #include "mv_device.cuh"
 #include "mv_internal.h"
 
@@ -441,3 +445,163 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
 }
 
 }  // namespace mv
+
+// ===================================================================== no-alloc
+// vis_fourier_slice_sum_noalloc: the direct slice sum of one group (the work
+// vis_fourier_volume_rendering does per group, including the C2R arrangement)
+// for callers that cannot allocate device memory: code that must keep a fixed
+// device-memory footprint, renders inside a frame loop where a cudaMalloc (and
+// the device-wide synchronisation a cudaFree implies) is not acceptable, or
+// runs under another framework's memory pool.  The caller passes every input
+// and output buffer; the split-K partial sums and the Phi^ table this kernel
+// needs live in the file-scope array below instead of a workspace.
+namespace mv {
+namespace {
+
+// Scratch of the no-alloc entry point: 8 MiB, held by every GPU that loads the
+// library until the process exits.  Its size bounds the slice:
+// (number of slice samples, rounded up to 8 in x) <= ~1.04 M.
+constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+std::map<int, void*> g_noalloc_address;  // device -> device address of g_noalloc_scratch
+
+// Device address of the scratch array on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device with cudaGetSymbolAddress (the first call on a device does this).
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    int st = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != kOk) return st;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    auto it = g_noalloc_address.find(dev);
+    if (it == g_noalloc_address.end()) {
+        void* p = nullptr;
+        st = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+        if (st != kOk) return st;
+        it = g_noalloc_address.emplace(dev, p).first;
+    }
+    *out = it->second;
+    return kOk;
+}
+
+}  // namespace
+}  // namespace mv
+
+extern "C" int vis_fourier_slice_sum_noalloc(const Constraint* d_constraints, const float* d_radii,
+                                             int number_of_terms, BasisFunctionId basis_function_id,
+                                             float2 step_size, int2 cutoff_frequency, float3 u_axis, float3 v_axis,
+                                             int2 number_of_samples, float2* d_arranged, int accumulate,
+                                             cudaStream_t stream) {
+    using namespace mv;
+    const int cx = cutoff_frequency.x, cy = cutoff_frequency.y;
+    const int nx = number_of_samples.x, ny = number_of_samples.y;
+    const int basis = (int)basis_function_id;
+    if (number_of_terms < 0 || (number_of_terms > 0 && !d_constraints) || !d_arranged)
+        return set_error(kInvalidValue, "vis_fourier_slice_sum_noalloc: NULL buffer or negative number of terms");
+    if (basis < 0 || basis >= kBasisCount) return set_error(kInvalidValue, "vis_fourier_slice_sum_noalloc: unknown basis");
+    if (cx < 0 || cy < 0 || nx < 1 || ny < 2 || 2 * cx > nx || 2 * cy > ny)
+        return set_error(kInvalidConfig, "vis_fourier_slice_sum_noalloc: cutoff_frequency does not fit number_of_samples");
+
+    // The lattice of vis_fourier_volume_rendering: x in (-cx, cx), y in [0, cy).
+    Lattice lat{};
+    lat.x0 = -cx + 1;
+    lat.nx = cx > 0 ? 2 * cx - 1 : 0;
+    lat.y0 = 0;
+    lat.ny = cy;
+    lat.z0 = 0;
+    lat.nz = 1;
+    lat.kx = step_size.x;
+    lat.ky = step_size.y;
+    lat.kz = 0.0;
+    const double sx = step_size.x, sy = step_size.y;
+    const double m[9] = {sx * u_axis.x, sx * u_axis.y, sx * u_axis.z, sy * v_axis.x, sy * v_axis.y, sy * v_axis.z,
+                         0.0, 0.0, 0.0};
+    for (int i = 0; i < 9; ++i) lat.m[i] = m[i];
+    if (lat.nx == 0 || lat.ny == 0) return kOk;
+
+    void* scratch = nullptr;
+    int st = noalloc_scratch(&scratch);
+    if (st != kOk) return st;
+
+    const bool factored = d_radii == nullptr;
+    const int amp = factored ? kAmpFactored : (basis == kSph || basis == kWendland) ? kAmpTable : kAmpExp2;
+    const int L = lat.nx >= 8 ? 8 : 1;
+    const int nxc = (lat.nx + L - 1) / L;
+    const long long n_rest = (long long)lat.ny;
+    const size_t plane = (size_t)nxc * L * n_rest;
+    // Without a radius maximum the table covers the full kMaxTable cells.
+    const int table_n = amp == kAmpTable ? kMaxTable : 0;
+    const double ds = amp == kAmpTable ? table_cell(basis) : 0.0;
+    const size_t table_bytes = amp == kAmpTable ? ((size_t)(table_n + 1) * sizeof(float4) + 255) / 256 * 256 : 0;
+    if (table_bytes + plane * sizeof(float2) > kNoAllocScratchBytes)
+        return set_error(kInvalidValue, "vis_fourier_slice_sum_noalloc: slice of " + std::to_string(plane) +
+                                            " samples exceeds the no-alloc scratch (" +
+                                            std::to_string((kNoAllocScratchBytes - table_bytes) / sizeof(float2)) +
+                                            " samples at most)");
+    const long long max_by_scratch = (long long)((kNoAllocScratchBytes - table_bytes) / (plane * sizeof(float2)));
+
+    const long long threads = (long long)nxc * n_rest;
+    const long long blocks_f = (threads + kThreads - 1) / kThreads;
+    const long long target = (long long)device_sm_count() * 6;
+    const long long max_splits = std::max<long long>(1, (number_of_terms + 4 * kThreads - 1) / (4 * kThreads));
+    long long splits = std::min<long long>(std::max<long long>(1, (target + blocks_f - 1) / blocks_f), max_splits);
+    splits = std::min<long long>(std::min<long long>(splits, max_by_scratch), 65535);
+    const long long chunk =
+        number_of_terms > 0 ? ((number_of_terms + splits - 1) / splits + kThreads - 1) / kThreads * kThreads : kThreads;
+    splits = number_of_terms > 0 ? (number_of_terms + chunk - 1) / chunk : 1;
+
+    // Scratch layout: [Phi^ table | split-K partials].  Every element the
+    // kernels read is written earlier in the same call, so the previous
+    // call's contents never matter and nothing needs clearing.
+    SumKernelArgs a;
+    a.particles = reinterpret_cast<const float4*>(d_constraints);
+    a.radii = d_radii;
+    a.n = number_of_terms;
+    a.chunk = (int)chunk;
+    a.lat = lat;
+    a.nxc = nxc;
+    a.n_rest = (int)n_rest;
+    a.table = reinterpret_cast<const float4*>(scratch);
+    a.table_n = table_n;
+    a.partial = reinterpret_cast<float2*>(static_cast<unsigned char*>(scratch) + table_bytes);
+    a.inv_ds = ds > 0 ? (float)(1.0 / ds) : 0.f;
+    a.amp_scale = basis == kGaussian ? kPiLog2e : -kPiLog2e;
+
+    if (amp == kAmpTable) {
+        phi_table_kernel<<<(table_n + 128) / 128, 128, 0, stream>>>(basis, ds, table_n, const_cast<float4*>(a.table));
+        count_launch();
+    }
+    SumKernel k = (L == 8) ? pick<8>(basis, amp) : pick<1>(basis, amp);
+    const size_t dyn_smem = amp == kAmpTable ? (size_t)(table_n + 1) * sizeof(float4) : 0;
+    if (dyn_smem > 48 * 1024) {
+        st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
+                        "cudaFuncSetAttribute");
+        if (st != kOk) return st;
+    }
+    k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, dyn_smem, stream>>>(a);
+    count_launch();
+    st = check_cuda(cudaGetLastError(), "plain_sum_kernel launch (no-alloc)");
+    if (st != kOk) return st;
+
+    FinalizeArgs f;
+    f.partial = a.partial;
+    f.splits = (int)splits;
+    f.plane = plane;
+    f.n_rest = (int)n_rest;
+    f.lat = lat;
+    f.basis = basis;
+    f.factored = factored;
+    f.scale = (double)step_size.x * (double)step_size.y;
+    f.out = d_arranged;
+    f.out_base = 0;
+    f.out_sx = f.out_sy = f.out_sz = 0;
+    f.wrap = nx;
+    f.row = ny / 2 + 1;
+    f.accumulate = accumulate != 0;
+    const long long count = (long long)lat.nx * n_rest;
+    finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(f);
+    count_launch();
+    return check_cuda(cudaGetLastError(), "finalize_kernel launch (no-alloc)");
+}
