@@ -84,6 +84,24 @@ def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
     return r
 
 
+def max_over_ranks(x, dist, device):
+    """Largest value of x over all ranks (the job's time is its slowest
+    rank's); x itself when there is no process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank_step, steps, t_max_ms, world):
+    """Whole-job throughput of `world` independent replicas, each processing
+    units_per_rank_step per step, timed by the slowest rank."""
+    return world * units_per_rank_step * steps / (t_max_ms / 1000.0)
+
+
 def compare_forms(M, cfg, sp, ds, w, stream, flush, args, steps=2):
     """The spectrum sum alone, tensor form vs plain form, same inputs."""
     import torch
@@ -295,11 +313,7 @@ def run_ours(args):
             dist.barrier()
 
     def allmax(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dist, "cuda")
 
     from libmeshlessvis_b200 import meshless as M
 
@@ -352,9 +366,8 @@ def run_ours(args):
     stage_t = {st: cfg.kernel_time(st) for st in STAGES}
     cfg.enable_timing(False)
     t_max = allmax(t_ms)
-    sec = t_max / 1000.0
-    value = world * terms * args.steps / sec / 1e9
-    views_per_s = world * nv * args.steps / sec
+    value = replica_throughput(terms, args.steps, t_max, world) / 1e9
+    views_per_s = replica_throughput(nv, args.steps, t_max, world)
 
     peaks, peak_src = measured_peaks()
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
