@@ -172,7 +172,7 @@ struct ConfigState {
     Workspace arranged;  // batched C2R inputs of vis_spectrum_render_views
     Workspace images;    // library-owned batched images
     Workspace views;     // per-view parameters
-    Workspace acc64;     // FP64 accumulators of the tensor-core form
+    TensorWorkspace tensor;  // tensor-core form: particle constants, FP64 accumulators, tables
     Workspace error_word;  // device int set by kernels that give up a bounded wait
     std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
     KernelTimer timer;
@@ -183,7 +183,7 @@ struct ConfigState {
         arranged.release();
         images.release();
         views.release();
-        acc64.release();
+        tensor.release();
         error_word.release();
         for (auto& kv : batched_plans) cufftDestroy(kv.second);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -673,10 +673,45 @@ struct VisSpectrum {
     size_t count;
 };
 
-namespace mv {
-int tensor_sum_available(const SumRequest& req);  // mv_tc_sum.cu
-int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, KernelTimer* timer);
-}  // namespace mv
+namespace {
+
+// The sum request of one registered group over a half-spectrum lattice
+// (accumulating into the spectrum).
+SumRequest spectrum_request(const VisSpectrum* sp, const Group& grp, ConfigState* s) {
+    SumRequest r{};
+    r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
+    r.radii = grp.d_radii;
+    const GroupStats gs = registered_group_stats(grp.d_constraints);
+    r.radius_min = gs.radius_min;
+    r.radius_max = gs.radius_max;
+    r.weight_max = gs.weight_max;
+    r.n = grp.number_of_terms;
+    r.basis = (int)grp.basis_function_id;
+    r.lat.x0 = -sp->grid.x / 2;
+    r.lat.nx = sp->grid.x;
+    r.lat.y0 = -sp->grid.y / 2;
+    r.lat.ny = sp->grid.y;
+    r.lat.z0 = 0;
+    r.lat.nz = sp->grid.z / 2 + 1;
+    r.lat.kx = r.lat.ky = r.lat.kz = sp->step;
+    const double st = sp->step;
+    const double m[9] = {st, 0, 0, 0, st, 0, 0, 0, st};
+    std::memcpy(r.lat.m, m, sizeof(m));
+    r.scale = 1.0;
+    r.out = sp->data;
+    r.out_base = 0;
+    r.out_sx = (long long)sp->grid.y * (sp->grid.z / 2 + 1);
+    r.out_sy = sp->grid.z / 2 + 1;
+    r.out_sz = 1;
+    r.wrap = 0;
+    r.row = 0;
+    r.accumulate = true;
+    r.stream = s->stream;
+    r.error_flag = static_cast<int*>(s->error_word.ptr);
+    return r;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -714,48 +749,31 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
     if (!sp || !s || !ds || (ds->number_of_groups > 0 && !ds->groups))
         return set_error(kInvalidValue, "vis_spectrum_compute: NULL or unknown argument");
     if (form < VIS_FORM_AUTO || form > VIS_FORM_TENSOR) return set_error(kInvalidValue, "vis_spectrum_compute: bad form");
-    if (ds->number_of_groups == 0)
-        return check_cuda(cudaMemsetAsync(sp->data, 0, sizeof(float2) * sp->count, s->stream), "cudaMemsetAsync");
+    std::vector<SumRequest> tc_groups, plain_groups;
     for (int g = 0; g < ds->number_of_groups; ++g) {
         const Group& grp = ds->groups[g];
         if (grp.number_of_terms > 0 && !grp.d_constraints)
             return set_error(kNotRegistered, "vis_spectrum_compute: group not registered");
-        SumRequest r{};
-        r.particles = reinterpret_cast<const float4*>(grp.d_constraints);
-        r.radii = grp.d_radii;
-        {
-            const GroupStats gs = registered_group_stats(grp.d_constraints);
-            r.radius_min = gs.radius_min;
-            r.radius_max = gs.radius_max;
-            r.weight_max = gs.weight_max;
-        }
-        r.error_flag = static_cast<int*>(s->error_word.ptr);
-        r.n = grp.number_of_terms;
-        r.basis = (int)grp.basis_function_id;
-        r.lat.x0 = -sp->grid.x / 2;
-        r.lat.nx = sp->grid.x;
-        r.lat.y0 = -sp->grid.y / 2;
-        r.lat.ny = sp->grid.y;
-        r.lat.z0 = 0;
-        r.lat.nz = sp->grid.z / 2 + 1;
-        r.lat.kx = r.lat.ky = r.lat.kz = sp->step;
-        const double st = sp->step;
-        const double m[9] = {st, 0, 0, 0, st, 0, 0, 0, st};
-        std::memcpy(r.lat.m, m, sizeof(m));
-        r.scale = 1.0;
-        r.out = sp->data;
-        r.out_base = 0;
-        r.out_sx = (long long)sp->grid.y * (sp->grid.z / 2 + 1);
-        r.out_sy = sp->grid.z / 2 + 1;
-        r.out_sz = 1;
-        r.wrap = 0;
-        r.row = 0;
-        r.accumulate = g > 0;
-        r.stream = s->stream;
-        int rc;
+        SumRequest r = spectrum_request(sp, grp, s);
         const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
-        if (want_tc && tensor_sum_available(r)) rc = launch_tensor_sum(r, s->partials, s->acc64, &s->timer);
-        else rc = launch_plain_sum(r, s->partials, &s->timer);
+        if (want_tc && tensor_sum_available(r)) tc_groups.push_back(r);
+        else plain_groups.push_back(r);
+    }
+    // every group adds into a zeroed spectrum (the result equals the
+    // reference's first-group-assigns, later-groups-accumulate)
+    int rc = check_cuda(cudaMemsetAsync(sp->data, 0, sizeof(float2) * sp->count, s->stream), "cudaMemsetAsync");
+    if (rc != kOk) return rc;
+    if (!tc_groups.empty()) {
+        TensorPlan plan;
+        rc = tensor_plan(tc_groups, plan);
+        if (rc == kOk) rc = tensor_reserve_upload(plan, s->tensor, s->stream);
+        if (rc == kOk)
+            rc = tensor_enqueue(tc_groups, plan, s->tensor, s->partials, &s->timer, s->stream,
+                                static_cast<int*>(s->error_word.ptr));
+        if (rc != kOk) return rc;
+    }
+    for (const SumRequest& r : plain_groups) {
+        rc = launch_plain_sum(r, s->partials, &s->timer);
         if (rc != kOk) return rc;
     }
     return kOk;

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -93,6 +94,77 @@ struct SliceRequest {
     cudaStream_t stream;
 };
 int launch_slice_extract(const SliceRequest& req, KernelTimer* timer);
+
+// Tensor-core form (mv_tc_sum.cu).  A set of groups -- of one or several
+// half-spectra -- is summed by one persistent tcgen05 launch:
+//   tensor_plan           host only: jobs, work items, accumulator classes;
+//   tensor_reserve_upload grows the workspaces and uploads the job and item
+//                         tables (not capturable in a CUDA graph);
+//   tensor_enqueue        memsets, per-particle constants, the persistent
+//                         launch, FP64 -> spectrum (added), Nyquist planes
+//                         (plain form, added); stream-ordered and capturable
+//                         once the workspaces are large enough.
+// The spectra must be zeroed (or hold earlier groups) before tensor_enqueue.
+int tensor_sum_available(const SumRequest& req);
+
+struct TcParticle;
+
+// One job of the persistent tensor-core kernel: a separable group summed over
+// a half-spectrum lattice into an FP64 accumulator.  Its work items are
+// (split ks, m tile, n tile), local index (ks * n_mtiles + m_tile) * n_ntiles
+// + n_tile.  Device-resident (64 bytes).
+struct TcJob {
+    const TcParticle* tp;  // the job's per-particle constants
+    double* acc;           // [(a_idx * ky + b_idx) * lz_tc + c][2]
+    double wmax;
+    int kx, ky, lz_tc;  // lattice extents; c planes [0, lz_tc) are summed here
+    int n_mtiles, n_ntiles;
+    int n;        // particles
+    int k_chunk;  // particles per item (multiple of 32)
+    int gauss;    // per-particle Gaussian factors (GAUSSIAN_DECAYING with radii)
+    int pad[2];
+};
+
+struct TensorPlan {
+    struct Class {
+        float2* out;
+        int kx, ky, lz_tc, lz_out;
+        double step;
+        int basis;
+        double h;
+        bool factored;
+        double scale;
+        size_t acc_offset;
+    };
+    std::vector<TcJob> jobs;
+    std::vector<int2> items;
+    std::vector<Class> classes;
+    std::vector<int> group_class, job_of_group;
+    std::vector<size_t> tp_offset;
+    size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
+    const void* d_jobs = nullptr;
+    const void* d_items = nullptr;
+};
+
+struct TensorWorkspace {
+    Workspace particles;  // per-particle constants of every group
+    Workspace acc;        // FP64 accumulators
+    Workspace meta;       // job and item tables
+    std::vector<char> uploaded;  // the tables last copied to `meta`
+    void* uploaded_to = nullptr;
+    void release() {
+        uploaded.clear();
+        uploaded_to = nullptr;
+        particles.release();
+        acc.release();
+        meta.release();
+    }
+};
+
+int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan);
+int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream);
+int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
+                   Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag);
 
 // Per-stage timing hooks (no-ops when timer == nullptr or disabled).
 void timer_begin(KernelTimer* timer, int stage, cudaStream_t stream);

@@ -57,11 +57,24 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 
 #include "mv_device.cuh"
 #include "mv_internal.h"
 
 namespace mv {
+
+// Per-particle constants of one group, computed once per launch by
+// tc_prep_kernel (48 bytes, three float4 loads).
+struct __align__(16) TcParticle {
+    uint32_t qx, qy, qz;  // fixed-point turns of step * position
+    float amp;            // 2^12 w / W
+    float gam;            // -pi log2(e) step^2 h^2 (GAUSSIAN_DECAYING), else 0
+    float rho2;           // exp2(2 gam): ratio of successive Gaussian step factors
+    float2 ry, rz;        // exp(-2 pi i Qy / 2^32), exp(-2 pi i Qz / 2^32), accurate
+    float pad[2];
+};
+static_assert(sizeof(TcParticle) == 48, "TcParticle layout");
 
 namespace {
 
@@ -94,29 +107,38 @@ constexpr size_t kSmemBytes = kBarrierOffset + 256;
 // idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, N = 128, M = 128.
 constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
 
-// Per-particle constants of one group, computed once per launch by
-// tc_prep_kernel (48 bytes, three float4 loads).
-struct __align__(16) TcParticle {
-    uint32_t qx, qy, qz;  // fixed-point turns of step * position
-    float amp;            // 2^12 w / W
-    float gam;            // -pi log2(e) step^2 h^2 (GAUSSIAN_DECAYING), else 0
-    float rho2;           // exp2(2 gam): ratio of successive Gaussian step factors
-    float2 ry, rz;        // exp(-2 pi i Qy / 2^32), exp(-2 pi i Qz / 2^32), accurate
-    float pad[2];
-};
-static_assert(sizeof(TcParticle) == kParticleBytes, "TcParticle layout");
 
 struct TcArgs {
-    const TcParticle* tp;
-    int k_begin, k_end;  // particle range of the group
-    int kx, ky, lz_tc;   // lattice extents; c planes [0, lz_tc) are summed here
-    int n_mtiles, n_ntiles;
-    int k_chunk;  // particles per work item (multiple of kKp)
-    int flush_stages;  // stages per TMEM accumulation chain (4 MMA K-steps each)
-    double wmax;
-    double* acc;  // [(a_idx * ky + b_idx) * lz_tc + c][2]
+    const TcJob* jobs;
+    const int2* items;  // (job, local item), longest first
+    int n_items;
+    int flush_stages;  // stages per TMEM accumulation chain (12 MMAs each)
     int* error_flag;
 };
+
+// Work of one item as every role sees it.
+struct TcItem {
+    const TcJob* job;
+    int m_tile, n_tile;
+    int kb, ke;
+    int n_stages, n_chunks;
+};
+
+__device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
+    const int2 v = a.items[it];
+    TcItem r;
+    r.job = a.jobs + v.x;
+    const int tiles = r.job->n_mtiles * r.job->n_ntiles;
+    const int ks = v.y / tiles;
+    const int ft = v.y % tiles;
+    r.m_tile = ft / r.job->n_ntiles;
+    r.n_tile = ft % r.job->n_ntiles;
+    r.kb = ks * r.job->k_chunk;
+    r.ke = min(r.job->n, r.kb + r.job->k_chunk);
+    r.n_stages = max(0, (r.ke - r.kb + kKp - 1) / kKp);
+    r.n_chunks = (r.n_stages + a.flush_stages - 1) / a.flush_stages;
+    return r;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -261,7 +283,11 @@ __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_secon
     return (h >> 16) | (h << 16);
 }
 
-template <bool GAUSS>
+// Persistent: CTA b walks items b, b + gridDim.x, ... of the longest-first
+// item list.  Every role walks the same items in the same order, and the
+// pipeline's stage and chunk counters (hence mbarrier phases and the TMEM
+// accumulator parity) run on across items; TMEM and the barriers are set up
+// once per CTA.
 __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* slots = smem + kStages * kStageBytes;  // [kStages][kSlotBytes]
@@ -278,17 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-
-    const int items_per_split = a.n_mtiles * a.n_ntiles;
-    const int ks = blockIdx.x / items_per_split;
-    const int ft = blockIdx.x % items_per_split;
-    const int m_tile = ft / a.n_ntiles;
-    const int n_tile = ft % a.n_ntiles;
-    const int kb = a.k_begin + ks * a.k_chunk;
-    const int ke = min(a.k_end, kb + a.k_chunk);
-    const int n_stages = max(0, (ke - kb + kKp - 1) / kKp);
     const int flush_stages = a.flush_stages;
-    const int n_chunks = (n_stages + flush_stages - 1) / flush_stages;
 
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
@@ -319,28 +335,34 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     if (warp == 0) {
         // ------------------------------------------------------------- MMA
         if (lane == 0) {
-            for (int s = 0; s < n_stages; ++s) {
-                const int buf = s % kStages;
-                const int k = s / flush_stages;
-                const int b = k & 1;
-                const bool first = (s % flush_stages) == 0;
-                if (first && k >= 2 && !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1, abort_flag, a.error_flag, 1))
-                    break;
-                if (!mbar_wait(&full[buf], (s / kStages) & 1, abort_flag, a.error_flag, 2)) break;
-                tc_fence_after();
-                const uint32_t base = smem_u32(smem + buf * kStageBytes);
-                const uint32_t a_hi = base, a_lo = base + kOperandBytes;
-                const uint32_t b_hi = base + 2 * kOperandBytes, b_lo = base + 3 * kOperandBytes;
-                const uint32_t d = tmem + (uint32_t)(b * kN);
+            int S = 0, C = 0;  // stages and chunks issued so far by this CTA
+            for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+                const TcItem I = tc_item(a, it);
+                for (int s = 0; s < I.n_stages; ++s, ++S) {
+                    const int buf = S % kStages;
+                    const int k = C + s / flush_stages;
+                    const int b = k & 1;
+                    const bool first = (s % flush_stages) == 0;
+                    if (first && k >= 2 &&
+                        !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1, abort_flag, a.error_flag, 1))
+                        break;
+                    if (!mbar_wait(&full[buf], (S / kStages) & 1, abort_flag, a.error_flag, 2)) break;
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(smem + buf * kStageBytes);
+                    const uint32_t a_hi = base, a_lo = base + kOperandBytes;
+                    const uint32_t b_hi = base + 2 * kOperandBytes, b_lo = base + 3 * kOperandBytes;
+                    const uint32_t d = tmem + (uint32_t)(b * kN);
 #pragma unroll
-                for (int t = 0; t < kKr / 16; ++t) {
-                    const uint32_t off = (uint32_t)(2 * t * kLbo);
-                    mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), (first && t == 0) ? 0u : 1u);
-                    mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), 1u);
-                    mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
+                    for (int t = 0; t < kKr / 16; ++t) {
+                        const uint32_t off = (uint32_t)(2 * t * kLbo);
+                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), (first && t == 0) ? 0u : 1u);
+                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), 1u);
+                        mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
+                    }
+                    mma_commit(&empty[buf]);
+                    if ((s % flush_stages) == flush_stages - 1 || s == I.n_stages - 1) mma_commit(&acc_full[b]);
                 }
-                mma_commit(&empty[buf]);
-                if ((s % flush_stages) == flush_stages - 1 || s == n_stages - 1) mma_commit(&acc_full[b]);
+                C += I.n_chunks;
             }
             mma_commit(drain);
         }
@@ -350,67 +372,81 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const int quarter = warp & 3;
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;  // M row owned by this thread
-        for (int k = 0; k < n_chunks; ++k) {
-            const int b = k & 1;
-            if (!mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4)) break;
-            tc_fence_after();
-            const bool last = k == n_chunks - 1;
+        int C = 0;
+        for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+            const TcItem I = tc_item(a, it);
+            const int lz_tc = I.job->lz_tc;
+            double* acc = I.job->acc;
+            const double wmax = I.job->wmax;
+            for (int kk = 0; kk < I.n_chunks; ++kk) {
+                const int k = C + kk;
+                const int b = k & 1;
+                if (!mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4)) break;
+                tc_fence_after();
+                const bool last = kk == I.n_chunks - 1;
 #pragma unroll 1
-            for (int cc = 0; cc < kN / 16; ++cc) {
-                float dv[16], tt[16], cp[16];
-                tmem_ld16(lane_base + b * kN + cc * 16, dv);
-                if (k > 0) {
-                    tmem_ld16(lane_base + kColTotal + cc * 16, tt);
-                    tmem_ld16(lane_base + kColComp + cc * 16, cp);
-                }
-                tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float v = dv[i] * kInvProductScale;
-                    if (k == 0) {
-                        tt[i] = v;
-                        cp[i] = 0.f;
-                    } else {
-                        const float y = v - cp[i];
-                        const float t = tt[i] + y;
-                        cp[i] = (t - tt[i]) - y;
-                        tt[i] = t;
+                for (int cc = 0; cc < kN / 16; ++cc) {
+                    float dv[16], tt[16], cp[16];
+                    tmem_ld16(lane_base + b * kN + cc * 16, dv);
+                    if (kk > 0) {
+                        tmem_ld16(lane_base + kColTotal + cc * 16, tt);
+                        tmem_ld16(lane_base + kColComp + cc * 16, cp);
                     }
-                }
-                if (!last) {
-                    tmem_st16(lane_base + kColTotal + cc * 16, tt);
-                    tmem_st16(lane_base + kColComp + cc * 16, cp);
-                } else {
-                    // add the item's total to the FP64 accumulator
-                    const int rho = m_tile * kM + row;
-                    const int c0 = n_tile * kNc;
+                    tmem_wait_ld();
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
-                        const int n = cc * 16 + i;
-                        const int c = c0 + (n % kNc);
-                        if (c < a.lz_tc) {
-                            const double v = ((double)tt[i] - (double)cp[i]) * a.wmax;
-                            atomicAdd(a.acc + ((size_t)rho * a.lz_tc + c) * 2 + (n / kNc), v);
+                        const float v = dv[i] * kInvProductScale;
+                        if (kk == 0) {
+                            tt[i] = v;
+                            cp[i] = 0.f;
+                        } else {
+                            const float y = v - cp[i];
+                            const float t = tt[i] + y;
+                            cp[i] = (t - tt[i]) - y;
+                            tt[i] = t;
+                        }
+                    }
+                    if (!last) {
+                        tmem_st16(lane_base + kColTotal + cc * 16, tt);
+                        tmem_st16(lane_base + kColComp + cc * 16, cp);
+                    } else {
+                        // add the item's total to the FP64 accumulator
+                        const int rho = I.m_tile * kM + row;
+                        const int c0 = I.n_tile * kNc;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const int n = cc * 16 + i;
+                            const int c = c0 + (n % kNc);
+                            if (c < lz_tc) {
+                                const double v = ((double)tt[i] - (double)cp[i]) * wmax;
+                                atomicAdd(acc + ((size_t)rho * lz_tc + c) * 2 + (n / kNc), v);
+                            }
                         }
                     }
                 }
+                tmem_wait_st();
+                tc_fence_before();
+                mbar_arrive(&acc_empty[b]);
             }
-            tmem_wait_st();
-            tc_fence_before();
-            mbar_arrive(&acc_empty[b]);
+            C += I.n_chunks;
         }
     } else if (warp == kLoaderWarp) {
         // ---------------------------------------------------------- loader
         if (lane == 0) {
-            for (int s = 0; s < n_stages; ++s) {
-                const int buf = s % kStages;
-                // the producers are done with this slot once stage s - kStages is full
-                if (s >= kStages && !mbar_wait(&full[buf], ((s / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
-                    break;
-                const int j0 = kb + s * kKp;
-                const uint32_t bytes = (uint32_t)(min(kKp, ke - j0) * kParticleBytes);
-                mbar_arrive_expect_tx(&pdata[buf], bytes);
-                bulk_copy_g2s(slots + buf * kSlotBytes, a.tp + j0, bytes, &pdata[buf]);
+            int S = 0;
+            for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+                const TcItem I = tc_item(a, it);
+                for (int s = 0; s < I.n_stages; ++s, ++S) {
+                    const int buf = S % kStages;
+                    // the producers are done with this slot once stage S - kStages is full
+                    if (S >= kStages &&
+                        !mbar_wait(&full[buf], ((S / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
+                        break;
+                    const int j0 = I.kb + s * kKp;
+                    const uint32_t bytes = (uint32_t)(min(kKp, I.ke - j0) * kParticleBytes);
+                    mbar_arrive_expect_tx(&pdata[buf], bytes);
+                    bulk_copy_g2s(slots + buf * kSlotBytes, I.job->tp + j0, bytes, &pdata[buf]);
+                }
             }
         }
         __syncwarp();
@@ -418,135 +454,139 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         // -------------------------------------------------------- producers
         const int p = tid - 32 * (1 + kFlushWarps);
         const int pp = p & 15;  // particle pair within the stage
-        // A unit (p < 256): 8-row chunk rc of the M tile
-        const bool has_a = p < 256;
+        const bool has_a = p < 256;  // A unit: 8-row chunk rc; else B unit: 8-column chunk cb
         const int rc = (p >> 4) & 15;
-        const int rho0 = m_tile * kM + rc * 8;
-        const int a_x = rho0 / a.ky - a.kx / 2;
-        const int b0 = rho0 % a.ky - a.ky / 2;
-        const bool a_up = b0 >= 0;
-        const int b_s = a_up ? b0 : b0 + 7;
-        // B unit (p >= 256): 8-column chunk cb of the N tile
         const int cb = (p >> 4) & 7;
-        const int c_s = n_tile * kNc + cb * 8;
-
-        for (int s = 0; s < n_stages; ++s) {
-            const int buf = s % kStages;
-            if (!mbar_wait(&pdata[buf], (s / kStages) & 1, abort_flag, a.error_flag, 64)) break;
-            uint32_t pqx[2], pqy[2], pqz[2];
-            float pamp[2], pgam[2], prho2[2];
-            float2 pry[2], prz[2];
+        int S = 0;
+        for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+            const TcItem I = tc_item(a, it);
+            const int kx = I.job->kx, ky = I.job->ky, lz_tc = I.job->lz_tc;
+            const bool gauss = I.job->gauss != 0;
+            const int rho0 = I.m_tile * kM + rc * 8;
+            const int a_x = rho0 / ky - kx / 2;
+            const int b0 = rho0 % ky - ky / 2;
+            const bool a_up = b0 >= 0;
+            const int b_s = a_up ? b0 : b0 + 7;
+            const int c_s = I.n_tile * kNc + cb * 8;
+            for (int s = 0; s < I.n_stages; ++s, ++S) {
+                const int buf = S % kStages;
+                if (!mbar_wait(&pdata[buf], (S / kStages) & 1, abort_flag, a.error_flag, 64)) break;
+                uint32_t pqx[2], pqy[2], pqz[2];
+                float pamp[2], pgam[2], prho2[2];
+                float2 pry[2], prz[2];
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int jj = 2 * pp + e;
-                if (kb + s * kKp + jj < ke) {
-                    const float4* src = reinterpret_cast<const float4*>(slots + buf * kSlotBytes + jj * kParticleBytes);
-                    const float4 v0 = src[0], v1 = src[1], v2 = src[2];
-                    pqx[e] = __float_as_uint(v0.x);
-                    pqy[e] = __float_as_uint(v0.y);
-                    pqz[e] = __float_as_uint(v0.z);
-                    pamp[e] = v0.w;
-                    pgam[e] = v1.x;
-                    prho2[e] = v1.y;
-                    pry[e] = make_float2(v1.z, v1.w);
-                    prz[e] = make_float2(v2.x, v2.y);
+                for (int e = 0; e < 2; ++e) {
+                    const int jj = 2 * pp + e;
+                    if (I.kb + s * kKp + jj < I.ke) {
+                        const float4* src =
+                            reinterpret_cast<const float4*>(slots + buf * kSlotBytes + jj * kParticleBytes);
+                        const float4 v0 = src[0], v1 = src[1], v2 = src[2];
+                        pqx[e] = __float_as_uint(v0.x);
+                        pqy[e] = __float_as_uint(v0.y);
+                        pqz[e] = __float_as_uint(v0.z);
+                        pamp[e] = v0.w;
+                        pgam[e] = v1.x;
+                        prho2[e] = v1.y;
+                        pry[e] = make_float2(v1.z, v1.w);
+                        prz[e] = make_float2(v2.x, v2.y);
+                    } else {
+                        pqx[e] = pqy[e] = pqz[e] = 0u;
+                        pamp[e] = 0.f;
+                        pgam[e] = 0.f;
+                        prho2[e] = 1.f;
+                        pry[e] = prz[e] = make_float2(1.f, 0.f);
+                    }
+                }
+                if (!mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)) break;
+                uint8_t* st = smem + buf * kStageBytes;
+                float2 z[2], R[2];
+                float q[2], rq[2];
+                if (has_a) {
+                    // ---- A: rows rc*8 .. rc*8+7, particles 2pp, 2pp+1 (amp includes 2^12)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        float sn, cs;
+                        __sincosf(turns_to_radians((uint32_t)a_x * pqx[e] + (uint32_t)b_s * pqy[e]), &sn, &cs);
+                        float g = pamp[e];
+                        R[e] = a_up ? pry[e] : make_float2(pry[e].x, -pry[e].y);
+                        if (gauss) {
+                            g *= exp2f(pgam[e] * (float)(a_x * a_x + b_s * b_s));
+                            q[e] = exp2f(pgam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
+                            rq[e] = prho2[e];
+                        } else {
+                            q[e] = 1.f;
+                            rq[e] = 1.f;
+                        }
+                        z[e] = make_float2(g * cs, -g * sn);
+                    }
+                    uint8_t* ahi = st;
+                    uint8_t* alo = st + kOperandBytes;
+                    const int col = (pp >> 1) * kLbo + rc * kCoreBytes + (pp & 1) * 8;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int r = a_up ? i : 7 - i;
+                        uint2 lo;
+                        const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
+                        *reinterpret_cast<uint2*>(ahi + col + r * 16) = hi;
+                        *reinterpret_cast<uint2*>(alo + col + r * 16) = lo;
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const float rx = R[e].x * q[e], ry = R[e].y * q[e];
+                            const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
+                            const float ny = fmaf(z[e].x, ry, z[e].y * rx);
+                            z[e] = make_float2(nx, ny);
+                            q[e] *= rq[e];
+                        }
+                    }
                 } else {
-                    pqx[e] = pqy[e] = pqz[e] = 0u;
-                    pamp[e] = 0.f;
-                    pgam[e] = 0.f;
-                    prho2[e] = 1.f;
-                    pry[e] = prz[e] = make_float2(1.f, 0.f);
-                }
-            }
-            if (!mbar_wait(&empty[buf], ((s / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)) break;
-            uint8_t* st = smem + buf * kStageBytes;
-            float2 z[2], R[2];
-            float q[2], rq[2];
-            if (has_a) {
-                // ---- A: rows rc*8 .. rc*8+7, particles 2pp, 2pp+1 (amp includes 2^12)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    float sn, cs;
-                    __sincosf(turns_to_radians((uint32_t)a_x * pqx[e] + (uint32_t)b_s * pqy[e]), &sn, &cs);
-                    float g = pamp[e];
-                    if constexpr (GAUSS) g *= exp2f(pgam[e] * (float)(a_x * a_x + b_s * b_s));
-                    z[e] = make_float2(g * cs, -g * sn);
-                    R[e] = a_up ? pry[e] : make_float2(pry[e].x, -pry[e].y);
-                    if constexpr (GAUSS) {
-                        q[e] = exp2f(pgam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
-                        rq[e] = prho2[e];
-                    } else {
-                        q[e] = 1.f;
-                        rq[e] = 1.f;
-                    }
-                }
-                uint8_t* ahi = st;
-                uint8_t* alo = st + kOperandBytes;
-                const int col = (pp >> 1) * kLbo + rc * kCoreBytes + (pp & 1) * 8;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const int r = a_up ? i : 7 - i;
-                    uint2 lo;
-                    const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                    *reinterpret_cast<uint2*>(ahi + col + r * 16) = hi;
-                    *reinterpret_cast<uint2*>(alo + col + r * 16) = lo;
+                    // ---- B: columns cb*8 .. cb*8+7 (Re) and 64 + ... (Im), scaled by 2^12
+                    const bool live = c_s < lz_tc;
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
-                        const float rx = R[e].x * q[e], ry = R[e].y * q[e];
-                        const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
-                        const float ny = fmaf(z[e].x, ry, z[e].y * rx);
-                        z[e] = make_float2(nx, ny);
-                        if constexpr (GAUSS) q[e] *= rq[e];
+                        float sn, cs;
+                        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
+                        float g = live ? kOperandScale : 0.f;
+                        R[e] = prz[e];
+                        if (gauss) {
+                            g *= exp2f(pgam[e] * (float)(c_s * c_s));
+                            q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
+                            rq[e] = prho2[e];
+                        } else {
+                            q[e] = 1.f;
+                            rq[e] = 1.f;
+                        }
+                        z[e] = make_float2(g * cs, -g * sn);
+                    }
+                    uint8_t* bhi = st + 2 * kOperandBytes;
+                    uint8_t* blo = st + 3 * kOperandBytes;
+                    const int kcol = (pp >> 1) * kLbo + (pp & 1) * 8;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        uint2 lo;
+                        const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
+                        const int re_off = kcol + cb * kCoreBytes + i * 16;
+                        const int im_off = kcol + (8 + cb) * kCoreBytes + i * 16;
+                        *reinterpret_cast<uint2*>(bhi + re_off) =
+                            make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
+                        *reinterpret_cast<uint2*>(blo + re_off) =
+                            make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
+                        *reinterpret_cast<uint2*>(bhi + im_off) =
+                            make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
+                        *reinterpret_cast<uint2*>(blo + im_off) =
+                            make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const float rx = R[e].x * q[e], ry = R[e].y * q[e];
+                            const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
+                            const float ny = fmaf(z[e].x, ry, z[e].y * rx);
+                            z[e] = make_float2(nx, ny);
+                            q[e] *= rq[e];
+                        }
                     }
                 }
-            } else {
-                // ---- B: columns cb*8 .. cb*8+7 (Re) and 64 + ... (Im), scaled by 2^12
-                const bool live = c_s < a.lz_tc;
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    float sn, cs;
-                    __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
-                    float g = live ? kOperandScale : 0.f;
-                    if constexpr (GAUSS) g *= exp2f(pgam[e] * (float)(c_s * c_s));
-                    z[e] = make_float2(g * cs, -g * sn);
-                    R[e] = prz[e];
-                    if constexpr (GAUSS) {
-                        q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
-                        rq[e] = prho2[e];
-                    } else {
-                        q[e] = 1.f;
-                        rq[e] = 1.f;
-                    }
-                }
-                uint8_t* bhi = st + 2 * kOperandBytes;
-                uint8_t* blo = st + 3 * kOperandBytes;
-                const int kcol = (pp >> 1) * kLbo + (pp & 1) * 8;
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    uint2 lo;
-                    const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                    const int re_off = kcol + cb * kCoreBytes + i * 16;
-                    const int im_off = kcol + (8 + cb) * kCoreBytes + i * 16;
-                    *reinterpret_cast<uint2*>(bhi + re_off) =
-                        make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
-                    *reinterpret_cast<uint2*>(blo + re_off) =
-                        make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
-                    *reinterpret_cast<uint2*>(bhi + im_off) =
-                        make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
-                    *reinterpret_cast<uint2*>(blo + im_off) =
-                        make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const float rx = R[e].x * q[e], ry = R[e].y * q[e];
-                        const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
-                        const float ny = fmaf(z[e].x, ry, z[e].y * rx);
-                        z[e] = make_float2(nx, ny);
-                        if constexpr (GAUSS) q[e] *= rq[e];
-                    }
-                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(&full[buf]);
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&full[buf]);
         }
     }
 
@@ -675,97 +715,216 @@ int tensor_sum_available(const SumRequest& r) {
     return separable ? 1 : 0;
 }
 
-int launch_tensor_sum(const SumRequest& req, Workspace& ws, Workspace& acc, KernelTimer* timer) {
-    const Lattice& L = req.lat;
-    const int kx = L.nx, ky = L.ny, lz_out = L.nz, lz_tc = L.nz - 1;
-    const bool uniform = req.radii && req.radius_min >= 0.f && req.radius_min == req.radius_max;
-    const bool gauss = req.radii && !uniform && req.basis == kGaussianDecaying;
-    const bool factored = !gauss;
-    const size_t acc_count = (size_t)kx * ky * lz_tc;
-    int st = acc.reserve(acc_count * 2 * sizeof(double));
-    if (st != kOk) return st;
-    st = check_cuda(cudaMemsetAsync(acc.ptr, 0, acc_count * 2 * sizeof(double), req.stream), "cudaMemsetAsync");
-    if (st != kOk) return st;
+namespace {
 
-    if (req.n > 0 && req.weight_max > 0.f) {
-        st = ws.reserve((size_t)req.n * sizeof(TcParticle));
-        if (st != kOk) return st;
-        TcPrepArgs pa;
-        pa.particles = req.particles;
-        pa.radii = req.radii;
-        pa.n = req.n;
-        pa.step = L.kx;
-        pa.gamma_scale = gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
-        pa.inv_wmax = 1.0f / req.weight_max;
-        pa.gauss = gauss;
-        pa.out = static_cast<TcParticle*>(ws.ptr);
-        tc_prep_kernel<<<(req.n + 255) / 256, 256, 0, req.stream>>>(pa);
-        count_launch();
-        st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
-        if (st != kOk) return st;
+// Groups that can share an FP64 accumulator: same output spectrum and the
+// same per-frequency factor (none for Gaussian jobs; Phi^(|k| h) with the
+// same basis and h for factored ones).
+struct ClassKey {
+    const float2* out;
+    int gauss;
+    int basis;
+    double h;
+    bool operator==(const ClassKey& o) const {
+        return out == o.out && gauss == o.gauss && (gauss || (basis == o.basis && h == o.h));
+    }
+};
 
-        TcArgs a;
-        a.tp = pa.out;
-        a.k_begin = 0;
-        a.k_end = req.n;
-        a.kx = kx;
-        a.ky = ky;
-        a.lz_tc = lz_tc;
-        a.n_mtiles = (int)((long long)kx * ky / kM);
-        a.n_ntiles = (lz_tc + kNc - 1) / kNc;
-        const long long ftiles = (long long)a.n_mtiles * a.n_ntiles;
-        // particle splits: enough items for ~4 waves, at least 64 stages each
+}  // namespace
+
+int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
+    plan = TensorPlan{};
+    std::vector<ClassKey> keys;
+    std::vector<std::pair<long long, int2>> items;  // (stages, item)
+    const int flush = tc_flush_stages();
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const SumRequest& r = groups[g];
+        const Lattice& L = r.lat;
+        const int kx = L.nx, ky = L.ny, lz_out = L.nz, lz_tc = L.nz - 1;
+        const bool uniform = r.radii && r.radius_min >= 0.f && r.radius_min == r.radius_max;
+        const bool gauss = r.radii && !uniform && r.basis == kGaussianDecaying;
+        ClassKey key{r.out, gauss ? 1 : 0, r.basis, uniform ? (double)r.radius_max : 1.0};
+        int cls = -1;
+        for (size_t c = 0; c < keys.size(); ++c)
+            if (keys[c] == key) cls = (int)c;
+        if (cls < 0) {
+            cls = (int)keys.size();
+            keys.push_back(key);
+            TensorPlan::Class c;
+            c.out = r.out;
+            c.kx = kx;
+            c.ky = ky;
+            c.lz_tc = lz_tc;
+            c.lz_out = lz_out;
+            c.step = L.kx;
+            c.basis = r.basis;
+            c.h = key.h;
+            c.factored = !gauss;
+            c.scale = r.scale;
+            c.acc_offset = plan.acc_bytes;
+            plan.acc_bytes += ((size_t)kx * ky * lz_tc * 2 * sizeof(double) + 255) / 256 * 256;
+            plan.classes.push_back(c);
+        }
+        plan.group_class.push_back(cls);
+        plan.tp_offset.push_back(plan.tp_bytes);
+        plan.tp_bytes += ((size_t)std::max(0, r.n) * sizeof(TcParticle) + 255) / 256 * 256;
+        if (r.n <= 0 || !(r.weight_max > 0.f)) {
+            plan.job_of_group.push_back(-1);
+            continue;
+        }
+        TcJob j{};
+        j.kx = kx;
+        j.ky = ky;
+        j.lz_tc = lz_tc;
+        j.n_mtiles = (int)((long long)kx * ky / kM);
+        j.n_ntiles = (lz_tc + kNc - 1) / kNc;
+        j.n = r.n;
+        j.gauss = gauss ? 1 : 0;
+        j.wmax = r.weight_max;
+        // particle splits: enough items per group for ~4 waves on its own, at
+        // least 64 stages each
+        const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
         const long long target = (long long)device_sm_count() * 4;
         long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
-        splits = std::min<long long>(splits, std::max<long long>(1, (req.n + 64 * kKp - 1) / (64 * kKp)));
-        long long chunk = ((req.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
-        splits = (req.n + chunk - 1) / chunk;
-        if (ftiles * splits > (1LL << 31) - 1) return set_error(kInvalidValue, "tensor sum: too many work items");
-        a.k_chunk = (int)chunk;
+        splits = std::min<long long>(splits, std::max<long long>(1, (r.n + 64 * kKp - 1) / (64 * kKp)));
+        const long long chunk = ((r.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
+        splits = (r.n + chunk - 1) / chunk;
+        j.k_chunk = (int)chunk;
+        const int job_index = (int)plan.jobs.size();
+        plan.job_of_group.push_back(job_index);
+        plan.jobs.push_back(j);
+        for (long long ks = 0; ks < splits; ++ks) {
+            const long long k0 = ks * chunk, k1 = std::min<long long>(r.n, k0 + chunk);
+            const long long stages = (k1 - k0 + kKp - 1) / kKp;
+            for (long long t = 0; t < ftiles; ++t)
+                items.push_back({stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+        }
+    }
+    if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
+    // longest first, then round-robin over the persistent CTAs
+    std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    plan.items.reserve(items.size());
+    for (auto& it : items) plan.items.push_back(it.second);
+    plan.meta_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256 + plan.items.size() * sizeof(int2);
+    return kOk;
+}
+
+int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream) {
+    int st = ws.particles.reserve(std::max<size_t>(plan.tp_bytes, 256));
+    if (st == kOk) st = ws.acc.reserve(std::max<size_t>(plan.acc_bytes, 256));
+    if (st == kOk) st = ws.meta.reserve(std::max<size_t>(plan.meta_bytes, 256));
+    if (st != kOk) return st;
+    char* tp_base = static_cast<char*>(ws.particles.ptr);
+    char* acc_base = static_cast<char*>(ws.acc.ptr);
+    for (size_t g = 0; g < plan.job_of_group.size(); ++g) {
+        const int j = plan.job_of_group[g];
+        if (j < 0) continue;
+        plan.jobs[j].tp = reinterpret_cast<const TcParticle*>(tp_base + plan.tp_offset[g]);
+        plan.jobs[j].acc = reinterpret_cast<double*>(acc_base + plan.classes[plan.group_class[g]].acc_offset);
+    }
+    std::vector<char> meta(plan.meta_bytes, 0);
+    const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
+    if (!plan.jobs.empty()) std::memcpy(meta.data(), plan.jobs.data(), plan.jobs.size() * sizeof(TcJob));
+    if (!plan.items.empty()) std::memcpy(meta.data() + jobs_bytes, plan.items.data(), plan.items.size() * sizeof(int2));
+    plan.d_jobs = static_cast<const void*>(ws.meta.ptr);
+    plan.d_items = static_cast<const void*>(static_cast<char*>(ws.meta.ptr) + jobs_bytes);
+    if (meta.empty()) return kOk;
+    // the same tables as last time (same groups, same buffers): nothing to copy
+    if (ws.uploaded_to == ws.meta.ptr && ws.uploaded == meta) return kOk;
+    st = check_cuda(cudaMemcpyAsync(ws.meta.ptr, meta.data(), meta.size(), cudaMemcpyHostToDevice, stream),
+                    "tensor metadata H2D");
+    if (st != kOk) return st;
+    // the host vector dies here: make sure the pageable copy has been staged
+    st = check_cuda(cudaStreamSynchronize(stream), "tensor metadata H2D");
+    if (st != kOk) return st;
+    ws.uploaded = std::move(meta);
+    ws.uploaded_to = ws.meta.ptr;
+    return kOk;
+}
+
+int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
+                   Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag) {
+    int st = kOk;
+    // zero the FP64 accumulators
+    if (plan.acc_bytes)
+        st = check_cuda(cudaMemsetAsync(ws.acc.ptr, 0, plan.acc_bytes, stream), "cudaMemsetAsync(acc)");
+    if (st != kOk) return st;
+    // per-particle constants of every group
+    for (size_t g = 0; g < groups.size(); ++g) {
+        const int j = plan.job_of_group[g];
+        if (j < 0) continue;
+        const SumRequest& r = groups[g];
+        const Lattice& L = r.lat;
+        TcPrepArgs pa;
+        pa.particles = r.particles;
+        pa.radii = r.radii;
+        pa.n = r.n;
+        pa.step = L.kx;
+        pa.gauss = plan.jobs[j].gauss != 0;
+        pa.gamma_scale = pa.gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
+        pa.inv_wmax = 1.0f / r.weight_max;
+        pa.out = const_cast<TcParticle*>(plan.jobs[j].tp);
+        tc_prep_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(pa);
+        count_launch();
+    }
+    st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
+    if (st != kOk) return st;
+    // one persistent launch for all groups
+    if (!plan.items.empty()) {
+        TcArgs a;
+        a.jobs = static_cast<const TcJob*>(plan.d_jobs);
+        a.items = static_cast<const int2*>(plan.d_items);
+        a.n_items = (int)plan.items.size();
         a.flush_stages = tc_flush_stages();
-        a.wmax = req.weight_max;
-        a.acc = static_cast<double*>(acc.ptr);
-        a.error_flag = req.error_flag;
-        auto kern = gauss ? tc_sum_kernel<true> : tc_sum_kernel<false>;
-        st = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes),
+        a.error_flag = error_flag;
+        st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kSmemBytes),
                         "cudaFuncSetAttribute");
         if (st != kOk) return st;
-        timer_begin(timer, 3, req.stream);
-        kern<<<(unsigned)(ftiles * splits), kThreads, kSmemBytes, req.stream>>>(a);
+        const int grid = std::min<int>(a.n_items, device_sm_count());
+        timer_begin(timer, 3, stream);
+        tc_sum_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
         count_launch();
-        timer_end(timer, 3, req.stream);
+        timer_end(timer, 3, stream);
         st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");
         if (st != kOk) return st;
     }
-
-    TcFinalizeArgs f;
-    f.acc = static_cast<const double*>(acc.ptr);
-    f.kx = kx;
-    f.ky = ky;
-    f.lz_tc = lz_tc;
-    f.lz_out = lz_out;
-    f.step = L.kx;
-    f.basis = req.basis;
-    f.h = uniform ? (double)req.radius_max : 1.0;
-    f.factored = factored;
-    f.scale = req.scale;
-    f.out = req.out;
-    f.accumulate = req.accumulate;
-    const long long count = (long long)acc_count;
-    tc_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, req.stream>>>(f);
-    count_launch();
+    // FP64 accumulators -> spectra (added to what is there)
+    for (const TensorPlan::Class& c : plan.classes) {
+        TcFinalizeArgs f;
+        f.acc = reinterpret_cast<const double*>(static_cast<const char*>(ws.acc.ptr) + c.acc_offset);
+        f.kx = c.kx;
+        f.ky = c.ky;
+        f.lz_tc = c.lz_tc;
+        f.lz_out = c.lz_out;
+        f.step = c.step;
+        f.basis = c.basis;
+        f.h = c.h;
+        f.factored = c.factored;
+        f.scale = c.scale;
+        f.out = c.out;
+        f.accumulate = true;
+        const long long count = (long long)c.kx * c.ky * c.lz_tc;
+        tc_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(f);
+        count_launch();
+    }
     st = check_cuda(cudaGetLastError(), "tc_finalize_kernel launch");
     if (st != kOk) return st;
-
-    // The Nyquist plane l = Kz/2 with the plain form.
-    SumRequest nyq = req;
-    nyq.lat.z0 = lz_tc;
-    nyq.lat.nz = 1;
-    nyq.out_base = lz_tc;
-    nyq.out_sx = (long long)ky * lz_out;
-    nyq.out_sy = lz_out;
-    nyq.out_sz = 1;
-    return launch_plain_sum(nyq, ws, nullptr);
+    // the Nyquist plane l = Kz/2 of every group with the plain form
+    for (const SumRequest& r : groups) {
+        SumRequest nyq = r;
+        const int lz_tc = r.lat.nz - 1;
+        nyq.lat.z0 = lz_tc;
+        nyq.lat.nz = 1;
+        nyq.out_base = lz_tc;
+        nyq.out_sx = (long long)r.lat.ny * r.lat.nz;
+        nyq.out_sy = r.lat.nz;
+        nyq.out_sz = 1;
+        nyq.accumulate = true;
+        st = launch_plain_sum(nyq, plain_ws, nullptr);
+        if (st != kOk) return st;
+    }
+    return kOk;
 }
 
 }  // namespace mv
