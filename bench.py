@@ -132,7 +132,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s"], default="c2",
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c4"], default="c2",
                    help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
                         "N=2^17, 128^3, 4 h-bins (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
@@ -456,10 +456,109 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """C4: 64 particle sets of uneven size and lattice, 16 views each, as one
+    batch (one CUDA graph per execute)."""
+    import torch
+
+    from libmeshlessvis_b200 import meshless as M
+    from libmeshlessvis_b200 import workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    form = {"auto": M.FORM_AUTO, "plain": M.FORM_PLAIN, "tensor": M.FORM_TENSOR}[args.form]
+    sets = W.c4()
+    lib = M.lib()
+    cfg = M.Config(block_length=64)
+    stream = torch.cuda.Stream()
+    cfg.set_stream(stream.cuda_stream)
+    terms = 0
+    n_total = 0
+    n_views = 0
+    datasets = []
+    batch = M.Batch(cfg)
+    for w in sets:
+        ds = M.Dataset(w["groups"])
+        cfg.register(ds)
+        datasets.append(ds)
+        t, n, g = terms_per_step(w)
+        terms += t
+        n_total += n
+        n_views += len(w["views"])
+        batch.add(ds, w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], [v[0] for v in w["views"]],
+                  [v[1] for v in w["views"]])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        batch.execute(form)
+    cfg.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(torch.cuda.current_device())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.vis_kernel_launch_count()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            batch.execute(form)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches_host = lib.vis_kernel_launch_count() - launches0
+    clk = clocks.stop()
+    t_max = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), dist, "cuda")
+    value = replica_throughput(terms, args.steps, t_max, world) / 1e9
+    uses_graph = batch.uses_graph()
+    # kernels per execute, counted on a direct (non-graph) run: graph replays
+    # launch the same nodes without passing through the library's host code
+    per_exec = launches_host / max(1, args.steps)
+    if uses_graph == 1:
+        probe = M.Batch(cfg)
+        for ds, w in zip(datasets, sets):
+            probe.add(ds, w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], [v[0] for v in w["views"]],
+                      [v[1] for v in w["views"]])
+        c0 = lib.vis_kernel_launch_count()
+        probe.execute(form)  # builds: one direct run + one capture of the same sequence
+        per_exec = (lib.vis_kernel_launch_count() - c0) / 2
+        probe.close()
+    batch.close()
+    for ds in datasets:
+        cfg.unregister(ds)
+    cfg.close()
+    if rank == 0:
+        line = {"metric": "GTerms/s (particle x frequency terms per second; batch of 64 uneven sets + all views)",
+                "value": value, "unit": "GTerms/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE config shapes)",
+                "config": {"workload": "C4", "sets": len(sets), "particles": n_total, "views": n_views,
+                           "form": args.form, "cuda_graph": uses_graph,
+                           "l2": "flushed between timed steps (256 MB write outside the event pair)",
+                           "parallelism": f"replicas x{world}"},
+                "views_per_s": replica_throughput(n_views, args.steps, t_max, world),
+                "clocks": clk, "gpu_launches": int(round(per_exec * args.steps))}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c4":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -96,6 +96,36 @@ int vis_spectrum_copy_to_host(VisSpectrum* spectrum, VisConfig* vis_config, floa
 int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int number_of_views,
                               const float3* u_axes, const float3* v_axes, float* d_images, float* h_images);
 
+/* ------------------------------------------------------------------ batch */
+/* A batch of jobs, each one registered dataset with its own half-spectrum
+ * lattice and its own views and image size (the reference renders one view of
+ * one dataset per call).  vis_batch_execute runs the whole batch as one CUDA
+ * graph on vis_config's stream: the spectra of every job -- one persistent
+ * tensor-core launch for every separable group of every job, the plain form
+ * for the rest -- then one slice-extraction launch for every view of every job,
+ * then one batched cuFFT C2R per distinct image size.  The first execute (and
+ * the first after vis_batch_add, or after a dataset was registered again)
+ * plans, reserves memory, runs once and captures the graph; later executes
+ * replay it.  Datasets must stay registered while the batch is used. */
+typedef struct VisBatch VisBatch;
+VisBatch* vis_batch_create(VisConfig* vis_config);
+/* Adds a job; returns its index (>= 0) or -VisError.  grid_size and
+ * spectrum_step as for vis_spectrum_create; view_step, cutoff_frequency and
+ * number_of_samples as in VisConfig; u_axes, v_axes: number_of_views float3
+ * each (copied). */
+int vis_batch_add(VisBatch* batch, MeshlessDataset* meshless_dataset, int3 grid_size, float spectrum_step,
+                  float2 view_step, int2 cutoff_frequency, int2 number_of_samples, int number_of_views,
+                  const float3* u_axes, const float3* v_axes);
+int vis_batch_execute(VisBatch* batch, int form);
+/* 1 if executes replay a captured CUDA graph, 0 if they launch directly (the
+ * capture failed), -1 before the first execute. */
+int vis_batch_uses_graph(VisBatch* batch);
+/* The job's images float[views][Nx][Ny] (device) and half-spectrum (device). */
+float* vis_batch_images(VisBatch* batch, int job);
+float2* vis_batch_spectrum(VisBatch* batch, int job);
+int vis_batch_copy_images_to_host(VisBatch* batch, int job, float* h_images);
+void vis_batch_destroy(VisBatch* batch);
+
 /* ----------------------------------------------------------------- timing */
 enum VisTimingStage
 {

@@ -112,6 +112,14 @@ SIGNATURES = {
     "vis_config_enable_kernel_timing": (c_int, [PConfig, c_int]),
     "vis_config_kernel_timing": (c_int, [PConfig, c_int, POINTER(c_float), POINTER(c_int)]),
     "vis_kernel_launch_count": (ctypes.c_ulonglong, []),
+    "vis_batch_create": (c_void_p, [PConfig]),
+    "vis_batch_add": (c_int, [c_void_p, PDataset, int3, c_float, float2, int2, int2, c_int, c_void_p, c_void_p]),
+    "vis_batch_execute": (c_int, [c_void_p, c_int]),
+    "vis_batch_uses_graph": (c_int, [c_void_p]),
+    "vis_batch_images": (c_void_p, [c_void_p, c_int]),
+    "vis_batch_spectrum": (c_void_p, [c_void_p, c_int]),
+    "vis_batch_copy_images_to_host": (c_int, [c_void_p, c_int, c_void_p]),
+    "vis_batch_destroy": (None, [c_void_p]),
     "vis_fourier_slice_sum_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, float2, int2, float3, float3, int2,
                                               c_void_p, c_int, c_void_p]),
 }

@@ -869,3 +869,284 @@ int vis_spectrum_render_views(VisSpectrum* sp, VisConfig* c, int number_of_views
 }
 
 }  // extern "C"
+
+// =================================================================== batch
+struct VisBatch {
+    VisConfig* cfg = nullptr;
+    struct Job {
+        MeshlessDataset* ds = nullptr;
+        VisSpectrum* sp = nullptr;
+        float2 view_step;
+        int2 cutoff, samples;
+        std::vector<float3> u, v;
+        int size_class = -1;
+        size_t image_offset = 0;  // floats into the class's image buffer
+    };
+    struct SizeClass {
+        int nx = 0, ny = 0, views = 0;
+        cufftHandle plan = 0;
+        Workspace arranged, images;
+    };
+    std::vector<Job> jobs;
+    std::vector<SizeClass> classes;
+    std::vector<SumRequest> tc_groups, plain_groups;
+    TensorPlan plan;
+    TensorWorkspace tensor;
+    Workspace partials, views_table;
+    int n_views = 0;
+    long long total_elements = 0;
+    std::vector<const void*> registered;  // device pointers the graph reads
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int mode = -1;  // -1 not built, 0 direct launches, 1 graph
+
+    void drop_build() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        for (SizeClass& c : classes) {
+            if (c.plan) cufftDestroy(c.plan);
+            c.arranged.release();
+            c.images.release();
+        }
+        classes.clear();
+        mode = -1;
+    }
+};
+
+namespace {
+
+std::vector<const void*> batch_pointers(const VisBatch* b) {
+    std::vector<const void*> out;
+    for (const VisBatch::Job& j : b->jobs)
+        for (int g = 0; g < j.ds->number_of_groups; ++g) {
+            out.push_back(j.ds->groups[g].d_constraints);
+            out.push_back(j.ds->groups[g].d_radii);
+            out.push_back(reinterpret_cast<const void*>((intptr_t)j.ds->groups[g].number_of_terms));
+        }
+    return out;
+}
+
+// Everything one execute enqueues; capturable once the workspaces are sized.
+int batch_enqueue(VisBatch* b, ConfigState* s) {
+    int rc = kOk;
+    for (const VisBatch::Job& j : b->jobs) {
+        rc = check_cuda(cudaMemsetAsync(j.sp->data, 0, sizeof(float2) * j.sp->count, s->stream), "cudaMemsetAsync");
+        if (rc != kOk) return rc;
+    }
+    int* err = static_cast<int*>(s->error_word.ptr);
+    if (!b->tc_groups.empty()) {
+        rc = tensor_enqueue(b->tc_groups, b->plan, b->tensor, b->partials, nullptr, s->stream, err);
+        if (rc != kOk) return rc;
+    }
+    for (const SumRequest& r : b->plain_groups) {
+        rc = launch_plain_sum(r, b->partials, nullptr);
+        if (rc != kOk) return rc;
+    }
+    rc = launch_slice_extract_batch(static_cast<const SliceView*>(b->views_table.ptr), b->n_views, b->total_elements,
+                                    s->stream, nullptr);
+    if (rc != kOk) return rc;
+    for (VisBatch::SizeClass& c : b->classes) {
+        rc = check_cufft(cufftSetStream(c.plan, s->stream), "cufftSetStream");
+        if (rc != kOk) return rc;
+        rc = check_cufft(cufftExecC2R(c.plan, static_cast<cufftComplex*>(c.arranged.ptr),
+                                      static_cast<float*>(c.images.ptr)),
+                         "cufftExecC2R (batch)");
+        if (rc != kOk) return rc;
+    }
+    return kOk;
+}
+
+int batch_build(VisBatch* b, ConfigState* s, int form) {
+    b->drop_build();
+    b->tc_groups.clear();
+    b->plain_groups.clear();
+    for (const VisBatch::Job& j : b->jobs)
+        for (int g = 0; g < j.ds->number_of_groups; ++g) {
+            const Group& grp = j.ds->groups[g];
+            if (grp.number_of_terms > 0 && !grp.d_constraints)
+                return set_error(kNotRegistered, "vis_batch_execute: a group of a batch dataset is not registered");
+            SumRequest r = spectrum_request(j.sp, grp, s);
+            const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
+            if (want_tc && tensor_sum_available(r)) b->tc_groups.push_back(r);
+            else b->plain_groups.push_back(r);
+        }
+    int rc = kOk;
+    if (!b->tc_groups.empty()) {
+        rc = tensor_plan(b->tc_groups, b->plan);
+        if (rc == kOk) rc = tensor_reserve_upload(b->plan, b->tensor, s->stream);
+        if (rc != kOk) return rc;
+    }
+    // image size classes, each rendered by one batched C2R
+    for (VisBatch::Job& j : b->jobs) {
+        int c = -1;
+        for (size_t k = 0; k < b->classes.size(); ++k)
+            if (b->classes[k].nx == j.samples.x && b->classes[k].ny == j.samples.y) c = (int)k;
+        if (c < 0) {
+            c = (int)b->classes.size();
+            b->classes.emplace_back();
+            b->classes.back().nx = j.samples.x;
+            b->classes.back().ny = j.samples.y;
+        }
+        j.size_class = c;
+        j.image_offset = (size_t)b->classes[c].views * j.samples.x * j.samples.y;
+        b->classes[c].views += (int)j.u.size();
+    }
+    std::vector<SliceView> views;
+    std::vector<int> class_done(b->classes.size(), 0);
+    long long elements = 0;
+    for (VisBatch::SizeClass& c : b->classes) {
+        const size_t per_arr = (size_t)c.nx * (c.ny / 2 + 1), per_img = (size_t)c.nx * c.ny;
+        rc = c.arranged.reserve(per_arr * c.views * sizeof(float2));
+        if (rc == kOk) rc = c.images.reserve(per_img * c.views * sizeof(float));
+        if (rc != kOk) return rc;
+        int n[2] = {c.nx, c.ny};
+        rc = check_cufft(cufftPlanMany(&c.plan, 2, n, nullptr, 1, (int)per_arr, nullptr, 1, (int)per_img, CUFFT_C2R,
+                                       c.views),
+                         "cufftPlanMany (batch)");
+        if (rc != kOk) return rc;
+    }
+    for (const VisBatch::Job& j : b->jobs) {
+        VisBatch::SizeClass& c = b->classes[j.size_class];
+        const size_t per_arr = (size_t)c.nx * (c.ny / 2 + 1);
+        for (size_t k = 0; k < j.u.size(); ++k) {
+            SliceView v{};
+            v.spectrum = j.sp->data;
+            v.arranged = static_cast<float2*>(c.arranged.ptr) + per_arr * class_done[j.size_class]++;
+            v.element_offset = elements;
+            v.gx = j.sp->grid.x;
+            v.gy = j.sp->grid.y;
+            v.gz = j.sp->grid.z;
+            v.inv_step = 1.0f / j.sp->step;
+            v.u[0] = j.u[k].x; v.u[1] = j.u[k].y; v.u[2] = j.u[k].z;
+            v.v[0] = j.v[k].x; v.v[1] = j.v[k].y; v.v[2] = j.v[k].z;
+            v.step[0] = j.view_step.x;
+            v.step[1] = j.view_step.y;
+            v.cx = j.cutoff.x;
+            v.cy = j.cutoff.y;
+            v.nx = j.samples.x;
+            v.ny = j.samples.y;
+            views.push_back(v);
+            elements += (long long)per_arr;
+        }
+    }
+    b->n_views = (int)views.size();
+    b->total_elements = elements;
+    if (!views.empty()) {
+        rc = b->views_table.reserve(views.size() * sizeof(SliceView));
+        if (rc == kOk)
+            rc = check_cuda(cudaMemcpyAsync(b->views_table.ptr, views.data(), views.size() * sizeof(SliceView),
+                                            cudaMemcpyHostToDevice, s->stream),
+                            "batch view table H2D");
+        if (rc == kOk) rc = check_cuda(cudaStreamSynchronize(s->stream), "batch view table H2D");
+        if (rc != kOk) return rc;
+    }
+    // one direct run sizes every workspace (and produces this execute's results)
+    rc = batch_enqueue(b, s);
+    if (rc != kOk) return rc;
+    rc = check_cuda(cudaStreamSynchronize(s->stream), "vis_batch_execute");
+    if (rc != kOk) return rc;
+    // capture the same sequence
+    b->mode = 0;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+        const int erc = batch_enqueue(b, s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+        if (erc == kOk && ce == cudaSuccess && g && cudaGraphInstantiate(&b->exec, g, 0) == cudaSuccess) {
+            b->graph = g;
+            b->mode = 1;
+        } else {
+            if (g) cudaGraphDestroy(g);
+            b->exec = nullptr;
+            vis_clear_last_error();
+        }
+    }
+    cudaGetLastError();
+    b->registered = batch_pointers(b);
+    return kOk;
+}
+
+}  // namespace
+
+extern "C" {
+
+VisBatch* vis_batch_create(VisConfig* vis_config) {
+    if (!vis_config || !state_of(vis_config)) {
+        set_error(kInvalidValue, "vis_batch_create: unknown config");
+        return nullptr;
+    }
+    VisBatch* b = new VisBatch();
+    b->cfg = vis_config;
+    return b;
+}
+
+int vis_batch_add(VisBatch* b, MeshlessDataset* ds, int3 grid_size, float spectrum_step, float2 view_step,
+                  int2 cutoff, int2 samples, int number_of_views, const float3* u_axes, const float3* v_axes) {
+    if (!b || !ds || (ds->number_of_groups > 0 && !ds->groups) || number_of_views < 0 ||
+        (number_of_views > 0 && (!u_axes || !v_axes)))
+        return -set_error(kInvalidValue, "vis_batch_add: NULL or bad argument");
+    if (cutoff.x < 0 || cutoff.y < 0 || samples.x < 1 || samples.y < 2 || 2 * cutoff.x > samples.x ||
+        2 * cutoff.y > samples.y)
+        return -set_error(kInvalidConfig, "vis_batch_add: cutoff/number_of_samples mismatch");
+    VisSpectrum* sp = vis_spectrum_create(grid_size, spectrum_step);
+    if (!sp) return -vis_get_last_error();
+    VisBatch::Job j;
+    j.ds = ds;
+    j.sp = sp;
+    j.view_step = view_step;
+    j.cutoff = cutoff;
+    j.samples = samples;
+    j.u.assign(u_axes, u_axes + number_of_views);
+    j.v.assign(v_axes, v_axes + number_of_views);
+    b->jobs.push_back(std::move(j));
+    b->drop_build();
+    return (int)b->jobs.size() - 1;
+}
+
+int vis_batch_execute(VisBatch* b, int form) {
+    ConfigState* s = b ? state_of(b->cfg) : nullptr;
+    if (!s) return set_error(kInvalidValue, "vis_batch_execute: unknown batch");
+    if (form < VIS_FORM_AUTO || form > VIS_FORM_TENSOR) return set_error(kInvalidValue, "vis_batch_execute: bad form");
+    if (b->mode < 0 || b->registered != batch_pointers(b)) return batch_build(b, s, form);
+    if (b->mode == 1) return check_cuda(cudaGraphLaunch(b->exec, s->stream), "cudaGraphLaunch");
+    return batch_enqueue(b, s);
+}
+
+int vis_batch_uses_graph(VisBatch* b) { return b ? b->mode : -1; }
+
+float* vis_batch_images(VisBatch* b, int job) {
+    if (!b || job < 0 || job >= (int)b->jobs.size() || b->jobs[job].size_class < 0 || b->mode < 0) return nullptr;
+    const VisBatch::Job& j = b->jobs[job];
+    return static_cast<float*>(b->classes[j.size_class].images.ptr) + j.image_offset;
+}
+
+float2* vis_batch_spectrum(VisBatch* b, int job) {
+    if (!b || job < 0 || job >= (int)b->jobs.size()) return nullptr;
+    return b->jobs[job].sp->data;
+}
+
+int vis_batch_copy_images_to_host(VisBatch* b, int job, float* h) {
+    ConfigState* s = b ? state_of(b->cfg) : nullptr;
+    float* d = vis_batch_images(b, job);
+    if (!s || !d || !h) return set_error(kInvalidValue, "vis_batch_copy_images_to_host: bad arguments");
+    const VisBatch::Job& j = b->jobs[job];
+    const size_t bytes = sizeof(float) * j.u.size() * j.samples.x * j.samples.y;
+    int rc = check_cuda(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s->stream), "batch images D2H");
+    if (rc != kOk) return rc;
+    return sync_and_check(s, "vis_batch_copy_images_to_host");
+}
+
+void vis_batch_destroy(VisBatch* b) {
+    if (!b) return;
+    ConfigState* s = state_of(b->cfg);
+    if (s) cudaStreamSynchronize(s->stream);
+    b->drop_build();
+    b->tensor.release();
+    b->partials.release();
+    b->views_table.release();
+    for (VisBatch::Job& j : b->jobs) vis_spectrum_destroy(j.sp);
+    delete b;
+}
+
+}  // extern "C"

@@ -95,6 +95,24 @@ struct SliceRequest {
 };
 int launch_slice_extract(const SliceRequest& req, KernelTimer* timer);
 
+// One view of a batched slice extraction: its spectrum, its image parameters
+// and where its C2R-layout slice goes.  Device-resident (96 bytes).
+struct SliceView {
+    const float2* spectrum;
+    float2* arranged;          // float2[nx][ny/2+1]
+    long long element_offset;  // prefix sum of nx*(ny/2+1) over the batch's views
+    int gx, gy, gz;            // the spectrum's lattice extents
+    float inv_step;            // 1 / spectral step
+    float u[3], v[3];
+    float step[2];
+    int cx, cy, nx, ny;
+    int pad;
+};
+// Slices of `number_of_views` views (descriptors in device memory) in one
+// launch; total_elements = sum over views of nx*(ny/2+1).
+int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, long long total_elements,
+                               cudaStream_t stream, KernelTimer* timer);
+
 // Tensor-core form (mv_tc_sum.cu).  A set of groups -- of one or several
 // half-spectra -- is summed by one persistent tcgen05 launch:
 //   tensor_plan           host only: jobs, work items, accumulator classes;

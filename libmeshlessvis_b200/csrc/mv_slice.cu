@@ -73,7 +73,71 @@ __global__ void slice_extract_kernel(SliceRequest r) {
     r.arranged[q] = out;
 }
 
+// Batched form: every view has its own spectrum and image size; thread q finds
+// its view by binary search over the views' element offsets.
+__global__ void slice_extract_batch_kernel(const SliceView* __restrict__ views, int n_views, long long total) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= total) return;
+    int lo = 0, hi = n_views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (views[mid].element_offset <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    const SliceView& V = views[lo];
+    const int h = V.ny / 2 + 1;
+    const int e = (int)(q - V.element_offset);
+    const int ix = e / h, y = e % h;
+
+    float2 out = make_float2(0.f, 0.f);
+    int x = 0;
+    bool valid = y < V.cy;
+    if (ix < V.cx) x = ix;
+    else if (ix > V.nx - V.cx) x = ix - V.nx;
+    else valid = false;
+
+    if (valid) {
+        const float fu = V.step[0] * (float)x, fv = V.step[1] * (float)y;
+        float p0 = (fu * V.u[0] + fv * V.v[0]) * V.inv_step;
+        float p1 = (fu * V.u[1] + fv * V.v[1]) * V.inv_step;
+        float p2 = (fu * V.u[2] + fv * V.v[2]) * V.inv_step;
+        const bool conj = p2 < 0.f;
+        if (conj) {
+            p0 = -p0;
+            p1 = -p1;
+            p2 = -p2;
+        }
+        const float f0 = floorf(p0), f1 = floorf(p1), f2 = floorf(p2);
+        const float t0 = p0 - f0, t1 = p1 - f1, t2 = p2 - f2;
+        const int i0 = (int)f0, j0 = (int)f1, l0 = (int)f2;
+        const int lz = V.gz / 2 + 1;
+        float re = 0.f, im = 0.f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int di = c & 1, dj = (c >> 1) & 1, dl = (c >> 2) & 1;
+            const float w = (di ? t0 : 1.f - t0) * (dj ? t1 : 1.f - t1) * (dl ? t2 : 1.f - t2);
+            const float2 s = corner(V.spectrum, V.gx, V.gy, lz, i0 + di, j0 + dj, l0 + dl);
+            re = fmaf(w, s.x, re);
+            im = fmaf(w, s.y, im);
+        }
+        const float scale = V.step[0] * V.step[1];
+        out = make_float2(re * scale, (conj ? -im : im) * scale);
+    }
+    V.arranged[e] = out;
+}
+
 }  // namespace
+
+int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, long long total_elements,
+                               cudaStream_t stream, KernelTimer* timer) {
+    if (number_of_views <= 0 || total_elements <= 0) return kOk;
+    timer_begin(timer, 1, stream);
+    slice_extract_batch_kernel<<<(unsigned)((total_elements + 255) / 256), 256, 0, stream>>>(d_views, number_of_views,
+                                                                                              total_elements);
+    count_launch();
+    timer_end(timer, 1, stream);
+    return check_cuda(cudaGetLastError(), "slice_extract_batch_kernel launch");
+}
 
 int launch_slice_extract(const SliceRequest& req, KernelTimer* timer) {
     const long long count = (long long)req.nx * (req.ny / 2 + 1) * req.number_of_views;

@@ -19,7 +19,7 @@ __all__ = ["get_simple_meshless_dataset", "delete_meshless_dataset", "delete_mes
            "get_number_of_terms", "load_meshless_datasets_from_file", "save_meshless_datasets_to_file",
            "shift_meshless_dataset", "Dataset", "Config", "Spectrum", "constraints_from_arrays", "VisError",
            "SPH", "GAUSSIAN", "WENDLAND_D3_C2", "GAUSSIAN_DECAYING", "FORM_AUTO", "FORM_PLAIN", "FORM_TENSOR",
-           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT", "STAGE_TENSOR_SUM"]
+           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT", "STAGE_TENSOR_SUM", "Batch"]
 
 
 def lib():
@@ -230,3 +230,76 @@ class Spectrum:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Owns a VisBatch*: jobs of (registered dataset, lattice, views), executed
+    as one CUDA graph (vis_batch_*)."""
+
+    def __init__(self, config):
+        self.lib = lib()
+        self.config = config
+        self.ptr = self.lib.vis_batch_create(config.ptr)
+        if not self.ptr:
+            L.check(self.lib)
+        self.jobs = []
+
+    def add(self, dataset, grid, spectrum_step, view_step, cutoff, samples, u_axes, v_axes):
+        u = np.ascontiguousarray(u_axes, dtype=np.float32).reshape(-1, 3)
+        v = np.ascontiguousarray(v_axes, dtype=np.float32).reshape(-1, 3)
+        j = self.lib.vis_batch_add(self.ptr, dataset.ref, int3(*grid), float(spectrum_step), float2(*view_step),
+                                   int2(*cutoff), int2(*samples), len(u), u.ctypes.data, v.ctypes.data)
+        if j < 0:
+            L.check(self.lib, -j)
+        self.jobs.append((tuple(grid), tuple(samples), len(u)))
+        return j
+
+    def execute(self, form=FORM_AUTO):
+        L.check(self.lib, self.lib.vis_batch_execute(self.ptr, int(form)))
+
+    def uses_graph(self):
+        return self.lib.vis_batch_uses_graph(self.ptr)
+
+    def images(self, job):
+        _, (nx, ny), nv = self.jobs[job]
+        out = np.empty((nv, nx, ny), dtype=np.float32)
+        L.check(self.lib, self.lib.vis_batch_copy_images_to_host(self.ptr, job, out.ctypes.data))
+        return out
+
+    def spectrum(self, job):
+        import ctypes as ct
+
+        (kx, ky, kz), _, _ = self.jobs[job]
+        out = np.empty((kx, ky, kz // 2 + 1), dtype=np.complex64)
+        d = self.lib.vis_batch_spectrum(self.ptr, job)
+        self.config.synchronize()
+        rt = _cudart()
+        assert rt.cudaMemcpy(out.ctypes.data, ct.c_void_p(d), out.nbytes, 2) == 0
+        return out
+
+    def close(self):
+        if self.ptr:
+            self.lib.vis_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _cudart():
+    """The CUDA runtime already loaded in this process (for plain device->host
+    copies of library-owned buffers)."""
+    import ctypes as ct
+
+    for name in ("libcudart.so.12", "/usr/local/cuda/lib64/libcudart.so"):
+        try:
+            rt = ct.CDLL(name)
+            rt.cudaMemcpy.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int]
+            rt.cudaMemcpy.restype = ct.c_int
+            return rt
+        except OSError:
+            continue
+    raise RuntimeError("CUDA runtime library not found")

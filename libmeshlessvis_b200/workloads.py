@@ -125,8 +125,8 @@ def c4(seed=0, sets=64, max_n=512 * 1024):
         w = rng.standard_normal(n).astype(np.float32) / np.sqrt(n)
         h = float(rng.uniform(0.01, 0.04))
         g = int(rng.choice([64, 96, 128, 192]))
-        # one h per set: no radii array, the set's h folds into the step
-        # (Phi^(|k| h) with |k| in units of the lattice step).
+        # one h per set, given as a constant radii array: Phi^(|k| h) then
+        # factors out of the sum (the tensor-core form applies it per frequency)
         out.append(dict(groups=[(constraints(pos, w), np.full(n, h, np.float32), WENDLAND_D3_C2)], grid=(g, g, g),
                         step3=1.0, cutoff=(g // 2, g // 2), samples=(g, g), views=rotating_views(16), step=(1.0, 1.0)))
     return out

@@ -281,3 +281,49 @@ def test_tensor_form_long_accumulation_random_points():
     got = spec_tc[ijk[:, 0] + 32, ijk[:, 1] + 32, ijk[:, 2]]
     assert O.rel_l2(got, ref) < SPEC_TOL
     assert O.rel_l2(spec_tc, spec_pl) < SPEC_TOL
+
+
+# ---------------------------------------------------------------- batching
+def test_batch_of_uneven_jobs_matches_fp64_and_replays_as_a_graph():
+    """Three jobs of different particle counts, bases, lattices and image sizes
+    (tensor-form and plain-form groups mixed) executed as one batch; each job's
+    spectrum and views match the FP64 oracle, and a second execute replaying
+    the captured CUDA graph gives the same images."""
+    rng = np.random.default_rng(41)
+    cfg = M.Config(cutoff=(8, 8), samples=(16, 16), block_length=64)
+    specs = [
+        # (n, basis, radii kind, grid, cutoff, samples, views)
+        (1500, M.WENDLAND_D3_C2, "uniform", (32, 32, 32), (16, 16), (32, 32), rotating_views(4)),
+        (777, M.GAUSSIAN_DECAYING, "per_particle", (48, 48, 32), (20, 24), (48, 48), rotating_views(3)),
+        (2048, M.SPH, "per_particle", (16, 16, 16), (8, 8), (16, 16), rotating_views(2)),  # plain form
+    ]
+    datasets, groups_of = [], []
+    for n, basis, kind, *_ in specs:
+        pos = rng.random((n, 3), dtype=np.float32)
+        w = rng.standard_normal(n).astype(np.float32)
+        radii = (np.full(n, 0.03, np.float32) if kind == "uniform"
+                 else np.exp(rng.uniform(np.log(0.01), np.log(0.05), n)).astype(np.float32))
+        groups = [(constraints(pos, w), radii, basis)]
+        groups_of.append(groups)
+        ds = to_dataset(groups)
+        cfg.register(ds)
+        datasets.append(ds)
+    batch = M.Batch(cfg)
+    for ds, (n, basis, kind, grid, cutoff, samples, views) in zip(datasets, specs):
+        batch.add(ds, grid, 1.0, (1.0, 1.0), cutoff, samples, [v[0] for v in views], [v[1] for v in views])
+    batch.execute(M.FORM_AUTO)
+    first = [batch.images(j) for j in range(len(specs))]
+    batch.execute(M.FORM_AUTO)
+    assert batch.uses_graph() == 1
+    for j, (groups, (n, basis, kind, grid, cutoff, samples, views)) in enumerate(zip(groups_of, specs)):
+        spec = batch.spectrum(j)
+        ref = O.spectrum_grid(groups, 1.0, grid)
+        assert O.rel_l2(spec, ref) < SPEC_TOL
+        imgs = batch.images(j)
+        ref_imgs = O.render_from_spectrum(ref, grid, 1.0, (1.0, 1.0), cutoff, views, samples)
+        assert O.rel_l2(imgs, ref_imgs) < IMAGE_TOL
+        np.testing.assert_array_equal(imgs, first[j])
+    batch.close()
+    for ds in datasets:
+        cfg.unregister(ds)
+    cfg.close()
