@@ -132,7 +132,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c4"], default="c2",
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c4", "c5"], default="c2",
                    help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
                         "N=2^17, 128^3, 4 h-bins (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
@@ -150,6 +150,9 @@ def workload(name):
         return W.c1()
     if name == "c3":
         return W.c3()
+    if name == "c5":
+        # the first frame of the 8-frame series (every frame has the same shapes)
+        return next(W.c5_frames())
     if name == "c3s":
         w = W.c3(n=1 << 17, grid=128, bins=4)
         w["name"] = "C3-small"
@@ -224,14 +227,16 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def cpu_baseline(w, sample_cutoff=(64, 64)):
+def cpu_baseline(w, target_terms=6e9):
     """The reference's own fourier_transform (OpenMP, all host threads) on the
-    workload's particles, for one slice of 2*cx*cy frequencies."""
+    workload's particles, for one slice of 2*cx*cy frequencies, cx = cy chosen
+    so the sample is about target_terms terms (at most 64)."""
     import oracle as O
 
     groups = w["groups"]
-    cx, cy = sample_cutoff
     n = sum(len(c) for c, _, _ in groups)
+    c = int(max(4, min(64, (target_terms / (2.0 * max(1, n))) ** 0.5)))
+    cx, cy = c, c
     terms = n * 2 * cx * cy
     cores = len(os.sched_getaffinity(0))
     if O.ref_available():

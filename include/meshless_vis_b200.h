@@ -126,6 +126,28 @@ float2* vis_batch_spectrum(VisBatch* batch, int job);
 int vis_batch_copy_images_to_host(VisBatch* batch, int job, float* h_images);
 void vis_batch_destroy(VisBatch* batch);
 
+/* -------------------------------------------------- image post-processing */
+/* Batches of images float[images][Nx][Ny] (device, as rendered) to RGB
+ * float[images][Nx][Ny][3] (device), on vis_config's stream. */
+/* vis_noninteractive/main.cpp:70-84: grey = max(sample, 0) / (max over the
+ * image's raw samples). */
+int vis_images_normalize_to_rgb(VisConfig* vis_config, const float* d_images, int number_of_images,
+                                int2 number_of_samples, float* d_rgb);
+/* vis_wx/local_glsl.h:28-87 (the viewer's display shader): clamp to
+ * [intensity_min, intensity_max] -> [0, 1], optional log scale, colour map
+ * 1 (fire), 2 (rainbow) or 3 (ice). */
+int vis_images_colormap(VisConfig* vis_config, const float* d_images, int number_of_images, int2 number_of_samples,
+                        float intensity_min, float intensity_max, int log_scale, int color_map, float* d_rgb);
+/* shift_meshless_dataset (include/meshless.h:66) applied to the registered
+ * device copy of every group, on vis_config's stream; the host arrays are not
+ * changed. */
+int vis_shift_registered_dataset(VisConfig* vis_config, MeshlessDataset* meshless_dataset, float x, float y,
+                                 float z);
+/* Writes one host RGB image (values clamped to [0, 1], 8 bits per channel) as a
+ * binary PPM, with the vertical flip the reference's JPEG writer applies
+ * (vis_noninteractive/main.cpp:29-35). */
+int vis_write_ppm(const char* filename, const float* h_rgb, int2 number_of_samples);
+
 /* ----------------------------------------------------------------- timing */
 enum VisTimingStage
 {

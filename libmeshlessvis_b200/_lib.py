@@ -120,6 +120,10 @@ SIGNATURES = {
     "vis_batch_spectrum": (c_void_p, [c_void_p, c_int]),
     "vis_batch_copy_images_to_host": (c_int, [c_void_p, c_int, c_void_p]),
     "vis_batch_destroy": (None, [c_void_p]),
+    "vis_images_normalize_to_rgb": (c_int, [PConfig, c_void_p, c_int, int2, c_void_p]),
+    "vis_images_colormap": (c_int, [PConfig, c_void_p, c_int, int2, c_float, c_float, c_int, c_int, c_void_p]),
+    "vis_write_ppm": (c_int, [c_char_p, c_void_p, int2]),
+    "vis_shift_registered_dataset": (c_int, [PConfig, PDataset, c_float, c_float, c_float]),
     "vis_fourier_slice_sum_noalloc": (c_int, [c_void_p, c_void_p, c_int, c_int, float2, int2, float3, float3, int2,
                                               c_void_p, c_int, c_void_p]),
 }

@@ -173,6 +173,7 @@ struct ConfigState {
     Workspace images;    // library-owned batched images
     Workspace views;     // per-view parameters
     TensorWorkspace tensor;  // tensor-core form: particle constants, FP64 accumulators, tables
+    Workspace post;          // image post-processing (per-image maxima)
     Workspace error_word;  // device int set by kernels that give up a bounded wait
     std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
     KernelTimer timer;
@@ -184,6 +185,7 @@ struct ConfigState {
         images.release();
         views.release();
         tensor.release();
+        post.release();
         error_word.release();
         for (auto& kv : batched_plans) cufftDestroy(kv.second);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -635,6 +637,25 @@ void vis_copy_to_host(VisConfig* c, float* h_image) {
 
 // ------------------------------------------------------------------ timing
 unsigned long long vis_kernel_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"
+
+namespace mv {
+// The config's stream and, when bytes > 0, a scratch buffer of the config.
+int config_stream_and_scratch(VisConfig* c, cudaStream_t* stream, void** scratch, size_t bytes) {
+    ConfigState* s = c ? state_of(c) : nullptr;
+    if (!s) return set_error(kInvalidValue, "unknown config");
+    *stream = s->stream;
+    if (bytes > 0) {
+        const int rc = s->post.reserve(bytes);
+        if (rc != kOk) return rc;
+        *scratch = s->post.ptr;
+    }
+    return kOk;
+}
+}  // namespace mv
+
+extern "C" {
 
 int vis_config_enable_kernel_timing(VisConfig* c, int enable) {
     ConfigState* s = c ? state_of(c) : nullptr;

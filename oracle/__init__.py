@@ -298,3 +298,51 @@ class RefRenderer:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Image post-processing (numpy restatements)
+# ---------------------------------------------------------------------------
+def normalize_to_rgb(images):
+    """vis_noninteractive/main.cpp:70-84: m = max over the raw samples (from
+    sample 0), negatives clamped to 0, grey RGB = sample / m."""
+    images = np.asarray(images, dtype=np.float64)
+    out = []
+    for img in images.reshape(images.shape[0], -1):
+        m = img.max()
+        g = np.maximum(img, 0.0) / m
+        out.append(np.repeat(g[:, None], 3, axis=1))
+    return np.stack(out).reshape(images.shape + (3,))
+
+
+_KNOTS = {
+    1: ([0.0, 0.475, 0.694, 0.745, 1.0], [(0, 0, 0), (0.686, 0.004, 0.0), (1.0, 0.42, 0.0), (1.0, 0.518, 0.0),
+                                          (1, 1, 1)]),
+    2: ([0.0, 0.25, 0.5, 0.75, 1.0], [(0, 0, 1), (0, 1, 1), (0, 1, 0), (1, 1, 0), (1, 0, 0)]),
+    3: ([0.0, 0.475, 0.694, 0.745, 1.0], [(0, 0, 0), (0.0, 0.004, 0.686), (0.0, 0.42, 1.0), (0.0, 0.518, 1.0),
+                                          (1, 1, 1)]),
+}
+
+
+def colormap(images, imin, imax, log_scale, color_map):
+    """vis_wx/local_glsl.h:28-87: a = max(0, (a-min)/(max-min)); log scale
+    (eps 1e-3, alpha 0.01); piecewise-linear map over 5 knots, the last colour
+    above the last knot."""
+    a = np.maximum(0.0, (np.asarray(images, dtype=np.float64) - imin) / (imax - imin))
+    if log_scale:
+        eps, alpha = 1e-3, 0.01
+        a = (-np.log(eps) + np.log(alpha * a + eps)) / (np.log(alpha + eps) - np.log(eps))
+    xs, cs = _KNOTS[color_map]
+    cs = np.asarray(cs, dtype=np.float64)
+    out = np.empty(a.shape + (3,))
+    flat = a.ravel()
+    res = out.reshape(-1, 3)
+    for idx, v in enumerate(flat):
+        col = cs[-1]
+        for i in range(1, 5):
+            if v <= xs[i]:
+                d = xs[i] - xs[i - 1]
+                col = ((v - xs[i - 1]) * cs[i] + (xs[i] - v) * cs[i - 1]) / d
+                break
+        res[idx] = col
+    return out

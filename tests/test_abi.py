@@ -155,3 +155,19 @@ def test_opengl_entry_point_reports_unsupported():
     lib.vis_opengl_fourier_volume_rendering(None, None, 1)
     assert lib.vis_get_last_error() == 7
     lib.vis_clear_last_error()
+
+
+def test_write_ppm_layout_and_flip(tmp_path):
+    lib = L.load()
+    w, h = 4, 3
+    rgb = np.zeros((h, w, 3), np.float32)
+    rgb[0, :, 0] = 1.0    # first row red
+    rgb[2, 1, 2] = 0.5    # last row, second pixel half blue
+    f = tmp_path / "img.ppm"
+    assert lib.vis_write_ppm(str(f).encode(), rgb.ctypes.data, L.int2(w, h)) == 0
+    data = f.read_bytes()
+    header = b"P6\n4 3\n255\n"
+    assert data.startswith(header)
+    px = np.frombuffer(data[len(header):], np.uint8).reshape(h, w, 3)
+    # vertical flip, as the reference's JPEG writer (vis_noninteractive/main.cpp:31)
+    assert (px[2, :, 0] == 255).all() and px[0, 1, 2] == 128

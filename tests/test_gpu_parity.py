@@ -327,3 +327,52 @@ def test_batch_of_uneven_jobs_matches_fp64_and_replays_as_a_graph():
     for ds in datasets:
         cfg.unregister(ds)
     cfg.close()
+
+
+# --------------------------------------------------------- post-processing
+@pytest.mark.parametrize("color_map,log_scale", [(1, 1), (2, 0), (3, 1)])
+def test_image_postprocessing_matches_restatement(color_map, log_scale):
+    import torch
+
+    rng = np.random.default_rng(51)
+    imgs = (rng.standard_normal((3, 24, 20)) * 5 + 2).astype(np.float32)
+    cfg = M.Config(cutoff=(8, 8), samples=(24, 20), block_length=64)
+    d_img = torch.from_numpy(imgs).cuda()
+    d_rgb = torch.empty((3, 24, 20, 3), dtype=torch.float32, device="cuda")
+    lib = M.lib()
+    from libmeshlessvis_b200 import _lib as L
+
+    rc = lib.vis_images_normalize_to_rgb(cfg.ptr, d_img.data_ptr(), 3, L.int2(24, 20), d_rgb.data_ptr())
+    assert rc == 0
+    cfg.synchronize()
+    np.testing.assert_allclose(d_rgb.cpu().numpy(), O.normalize_to_rgb(imgs), rtol=1e-6, atol=1e-7)
+    rc = lib.vis_images_colormap(cfg.ptr, d_img.data_ptr(), 3, L.int2(24, 20), -1.0, 9.0, log_scale, color_map,
+                                 d_rgb.data_ptr())
+    assert rc == 0
+    cfg.synchronize()
+    np.testing.assert_allclose(d_rgb.cpu().numpy(), O.colormap(imgs, -1.0, 9.0, log_scale, color_map),
+                               rtol=1e-5, atol=1e-6)
+    cfg.close()
+
+
+def test_device_shift_matches_host_shift():
+    """vis_noninteractive shifts every dataset by -5 before rendering
+    (vis_noninteractive/main.cpp:46); shifting the registered device copy gives
+    the same image as shifting on the host."""
+    rng = np.random.default_rng(61)
+    n = 900
+    pos = rng.random((n, 3), dtype=np.float32) * 10
+    cons = constraints(pos, rng.random(n, dtype=np.float32))
+    radii = np.full(n, 0.4, np.float32)
+    cfg = M.Config(step=(0.1, 0.1), cutoff=(16, 16), samples=(64, 64), block_length=64)
+    ds = to_dataset([(cons, radii, M.SPH)])
+    cfg.register(ds)
+    lib = M.lib()
+    assert lib.vis_shift_registered_dataset(cfg.ptr, ds.ref, -5.0, -5.0, -5.0) == 0
+    cfg.render(ds)
+    img = cfg.image()
+    cfg.unregister(ds)
+    cfg.close()
+    shifted = constraints(pos - np.float32(5.0), cons["weight"])
+    ref = O.render_direct([(shifted, radii, M.SPH)], (0.1, 0.1), (16, 16), (1, 0, 0), (0, 1, 0), (64, 64))
+    assert O.rel_l2(img, ref) < SPEC_TOL
