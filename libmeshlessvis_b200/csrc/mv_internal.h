@@ -125,14 +125,12 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 // The spectra must be zeroed (or hold earlier groups) before tensor_enqueue.
 int tensor_sum_available(const SumRequest& req);
 
-struct TcParticle;
-
 // One job of the persistent tensor-core kernel: a separable group summed over
 // a half-spectrum lattice into an FP64 accumulator.  Its work items are
 // (split ks, m tile, n tile), local index (ks * n_mtiles + m_tile) * n_ntiles
 // + n_tile.  Device-resident (64 bytes).
 struct TcJob {
-    const TcParticle* tp;  // the job's per-particle constants
+    const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
     double* acc;           // [(a_idx * ky + b_idx) * lz_tc + c][2]
     double wmax;
     int kx, ky, lz_tc;  // lattice extents; c planes [0, lz_tc) are summed here

@@ -224,6 +224,191 @@ __global__ void __launch_bounds__(kThreads, 2) plain_sum_kernel(SumKernelArgs a)
     for (int m = 0; m < L; ++m) out[(size_t)m * a.n_rest] = make_float2(tot[m].x - comp[m].x, tot[m].y - comp[m].y);
 }
 
+// Folded form: the lattice's x range holds 0 (and, with FY == 2, so does its
+// y range).  |k| and every Phi^ factor are even in x and in y, and the phase
+// at (-x, y, z) is that at (x, y, z) with the x part conjugated:
+//   e^{i n.Q} at (sx xp, sy yp, z) = c^{sx} d_{sy},  c = e^{i xp Qx},
+//   d_{+-} = w e^{i (+-yp Qy + z Qz)}.
+// A thread owns L representatives xp = xc L + m >= 0, one yp >= 0 (FY == 2;
+// FY == 1: one y of the lattice) and one z, and sums the terms at (+-xp, yp)
+// (and (+-xp, -yp)) together: one amplitude evaluation and one x rotation
+// serve up to four lattice points.  With u = amp c, the four real sums
+//   A0 = sum ur dr, A1 = sum ui di, A2 = sum ur di, A3 = sum ui dr
+// give T(+xp) = (A0 - A1, A2 + A3) and T(-xp) = (A0 + A1, A2 - A3).
+// Terms outside the lattice and the mirrors of xp = 0 / yp = 0 are computed
+// but not stored.  The partial-sum layout is the plain kernel's.
+struct FoldKernelArgs {
+    SumKernelArgs s;
+    int xpc;       // x chunks of L representatives: ceil(XP / L)
+    int yrows;     // FY == 2: YP representatives yp; FY == 1: lat.ny
+    size_t plane;  // partial sums per split: lat.nx * n_rest
+};
+
+template <int L, int FY, int AMP>
+__global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa) {
+    const SumKernelArgs& a = fa.s;
+    extern __shared__ float4 s_tab[];  // table cells (kAmpTable only)
+    __shared__ uint4 s_q[kThreads];    // Qx, Qy, Qz, weight bits
+    __shared__ float2 s_rot[kThreads];  // exp(2 pi i Qx / 2^32)
+    __shared__ float s_h[kThreads];    // per-particle amplitude parameter
+
+    const int tid = threadIdx.x;
+    if constexpr (AMP == kAmpTable) {
+        for (int i = tid; i <= a.table_n; i += kThreads) s_tab[i] = a.table[i];
+    }
+
+    const int nz = a.lat.nz;
+    const long long n_rest_f = (long long)fa.yrows * nz;
+    const long long t = (long long)blockIdx.x * kThreads + tid;
+    const bool active = t < (long long)fa.xpc * n_rest_f;
+    const int xc = active ? (int)(t / n_rest_f) : 0;
+    const int rf = active ? (int)(t % n_rest_f) : 0;
+    const int yp = FY == 2 ? rf / nz : a.lat.y0 + rf / nz;
+    const int z = a.lat.z0 + rf % nz;
+    const int xb = xc * L;
+
+    // |k| (kAmpTable) or |k|^2 (kAmpExp2) of the thread's L representatives.
+    float r[L];
+    if constexpr (AMP != kAmpFactored) {
+        const double ry = a.lat.ky * yp, rz = a.lat.kz * z;
+#pragma unroll
+        for (int m = 0; m < L; ++m) {
+            const double rx = a.lat.kx * (xb + m);
+            const double r2 = rx * rx + ry * ry + rz * rz;
+            r[m] = AMP == kAmpTable ? (float)sqrt(r2) : (float)r2;
+        }
+    }
+
+    constexpr int NS = 4 * FY;  // real sums per representative
+    float tot[L][NS], comp[L][NS];
+#pragma unroll
+    for (int m = 0; m < L; ++m)
+#pragma unroll
+        for (int i = 0; i < NS; ++i) tot[m][i] = comp[m][i] = 0.f;
+
+    const int beg = blockIdx.y * a.chunk;
+    const int end = min(a.n, beg + a.chunk);
+    const uint32_t uxb = (uint32_t)xb, uy = (uint32_t)yp, uz = (uint32_t)z;
+
+    for (int t0 = beg; t0 < end; t0 += kThreads) {
+        __syncthreads();
+        const int idx = t0 + tid;
+        if (idx < end) {
+            const float4 p = a.particles[idx];
+            const double px = p.x, py = p.y, pz = p.z;
+            const double* mm = a.lat.m;
+            const uint32_t qx = fixed_turns(mm[0] * px + mm[1] * py + mm[2] * pz);
+            s_q[tid] = make_uint4(qx, fixed_turns(mm[3] * px + mm[4] * py + mm[5] * pz),
+                                  fixed_turns(mm[6] * px + mm[7] * py + mm[8] * pz), __float_as_uint(p.w));
+            double sn, cs;
+            sincospi((double)(int32_t)qx * (1.0 / 2147483648.0), &sn, &cs);
+            s_rot[tid] = make_float2((float)cs, (float)sn);
+            if constexpr (AMP == kAmpTable) s_h[tid] = a.radii[idx] * a.inv_ds;
+            else if constexpr (AMP == kAmpExp2) {
+                const float h = a.radii[idx];
+                s_h[tid] = a.amp_scale * h * h;
+            }
+        }
+        __syncthreads();
+        const int cnt = min(kThreads, end - t0);
+
+        float acc[L][NS];
+#pragma unroll
+        for (int m = 0; m < L; ++m)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) acc[m][i] = 0.f;
+
+#pragma unroll 1
+        for (int j = 0; j < cnt; ++j) {
+            const uint4 q = s_q[j];
+            const float2 R = s_rot[j];
+            float hv = 0.f;
+            if constexpr (AMP != kAmpFactored) hv = s_h[j];
+            const float w = __uint_as_float(q.w);
+            const uint32_t pyz = uy * q.y + uz * q.z;
+            float sn, cs;
+            __sincosf(turns_to_radians(pyz), &sn, &cs);
+            const float dpr = w * cs, dpi = w * sn;
+            float dmr = 0.f, dmi = 0.f;
+            if constexpr (FY == 2) {
+                __sincosf(turns_to_radians(pyz - 2u * uy * q.y), &sn, &cs);
+                dmr = w * cs;
+                dmi = w * sn;
+            }
+            __sincosf(turns_to_radians(uxb * q.x), &sn, &cs);
+            float cr = cs, ci = sn;
+#pragma unroll
+            for (int m = 0; m < L; ++m) {
+                float ur = cr, ui = ci;
+                if constexpr (AMP != kAmpFactored) {
+                    float amp;
+                    if constexpr (AMP == kAmpTable) {
+                        const float u = r[m] * hv;  // s / ds
+                        const float tt = u + 12582912.0f;  // round to nearest cell (1.5 * 2^23)
+                        const unsigned k = min((unsigned)(__float_as_int(tt) - 0x4B400000), (unsigned)a.table_n);
+                        const float fr = u - (tt - 12582912.0f);
+                        const float4 c = s_tab[k];
+                        amp = fmaf(fmaf(fmaf(c.w, fr, c.z), fr, c.y), fr, c.x);
+                    } else {
+                        amp = exp2f(hv * r[m]);
+                    }
+                    ur *= amp;
+                    ui *= amp;
+                }
+                acc[m][0] = fmaf(ur, dpr, acc[m][0]);
+                acc[m][1] = fmaf(ui, dpi, acc[m][1]);
+                acc[m][2] = fmaf(ur, dpi, acc[m][2]);
+                acc[m][3] = fmaf(ui, dpr, acc[m][3]);
+                if constexpr (FY == 2) {
+                    acc[m][4] = fmaf(ur, dmr, acc[m][4]);
+                    acc[m][5] = fmaf(ui, dmi, acc[m][5]);
+                    acc[m][6] = fmaf(ur, dmi, acc[m][6]);
+                    acc[m][7] = fmaf(ui, dmr, acc[m][7]);
+                }
+                if (m + 1 < L) {
+                    const float nr = fmaf(cr, R.x, -ci * R.y);
+                    const float ni = fmaf(cr, R.y, ci * R.x);
+                    cr = nr;
+                    ci = ni;
+                }
+            }
+        }
+        // Kahan: add this tile's sums to the running totals.
+#pragma unroll
+        for (int m = 0; m < L; ++m)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) {
+                const float yv = acc[m][i] - comp[m][i];
+                const float tv = tot[m][i] + yv;
+                comp[m][i] = (tv - tot[m][i]) - yv;
+                tot[m][i] = tv;
+            }
+    }
+
+    if (!active) return;
+    float2* out = a.partial + blockIdx.y * fa.plane;
+    const int x_lo = a.lat.x0, x_hi = a.lat.x0 + a.lat.nx - 1;
+    const int y_lo = a.lat.y0, y_hi = a.lat.y0 + a.lat.ny - 1;
+#pragma unroll
+    for (int m = 0; m < L; ++m) {
+        float v[NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) v[i] = tot[m][i] - comp[m][i];
+        const int xp = xb + m;
+#pragma unroll
+        for (int sy = 0; sy < FY; ++sy) {
+            const int y = sy == 0 ? yp : -yp;
+            if (sy == 1 && yp == 0) continue;
+            if (y < y_lo || y > y_hi) continue;
+            const float* A = v + 4 * sy;
+            const size_t rest = (size_t)(y - y_lo) * nz + (z - a.lat.z0);
+            if (xp <= x_hi) out[(size_t)(xp - x_lo) * a.n_rest + rest] = make_float2(A[0] - A[1], A[2] + A[3]);
+            if (xp > 0 && -xp >= x_lo)
+                out[(size_t)(-xp - x_lo) * a.n_rest + rest] = make_float2(A[0] + A[1], A[2] - A[3]);
+        }
+    }
+}
+
 // Cubic pieces of Phi^ on cells [(k - 1/2) ds, (k + 1/2) ds]: the polynomial in
 // fr = s/ds - k interpolating Phi^ (FP64, reference branch points) at the four
 // Chebyshev points of the cell.  Cells never straddle a branch point because
@@ -322,6 +507,15 @@ SumKernel pick_amp(int amp) {
     else return plain_sum_kernel<L, BASIS, kAmpExp2>;
 }
 
+using FoldKernel = void (*)(FoldKernelArgs);
+
+template <int L, int FY>
+FoldKernel pick_fold(int amp) {
+    if (amp == kAmpFactored) return fold_sum_kernel<L, FY, kAmpFactored>;
+    if (amp == kAmpTable) return fold_sum_kernel<L, FY, kAmpTable>;
+    return fold_sum_kernel<L, FY, kAmpExp2>;
+}
+
 template <int L>
 SumKernel pick(int basis, int amp) {
     switch (basis) {
@@ -352,7 +546,15 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     const int L = lat.nx >= 8 ? 8 : 1;
     const int nxc = (lat.nx + L - 1) / L;
     const long long n_rest = (long long)lat.ny * lat.nz;
-    const long long threads = (long long)nxc * n_rest;
+    // Folded form when x = 0 is on the lattice (and y folds too when the y
+    // range holds both signs): L = 4 x representatives with y folded, else 8.
+    const bool fold = lat.x0 <= 0 && lat.x0 + lat.nx - 1 >= 0;
+    const bool fold_y = fold && lat.y0 < 0 && lat.y0 + lat.ny - 1 > 0;
+    const int fold_l = fold_y ? 4 : 8;
+    const int xp_count = std::max(-lat.x0, lat.x0 + lat.nx - 1) + 1;
+    const int yrows = fold_y ? std::max(-lat.y0, lat.y0 + lat.ny - 1) + 1 : lat.ny;
+    const int xpc = (xp_count + fold_l - 1) / fold_l;
+    const long long threads = fold ? (long long)xpc * yrows * lat.nz : (long long)nxc * n_rest;
     if (threads > (1LL << 31) - 1) return set_error(kInvalidValue, "lattice too large");
     const long long blocks_f = (threads + kThreads - 1) / kThreads;
 
@@ -381,7 +583,7 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         table_n = std::max(table_n, 1);
     }
 
-    const size_t plane = (size_t)nxc * L * n_rest;
+    const size_t plane = fold ? (size_t)lat.nx * n_rest : (size_t)nxc * L * n_rest;
     const size_t part_bytes = (plane * splits * sizeof(float2) + 255) / 256 * 256;
     const size_t table_cells = amp == kAmpTable ? (size_t)table_n + 1 : 0;
     int st = ws.reserve(part_bytes + table_cells * sizeof(float4));
@@ -407,18 +609,37 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         count_launch();
     }
 
-    SumKernel k = (L == 8) ? pick<8>(req.basis, amp) : pick<1>(req.basis, amp);
     const size_t dyn_smem = table_cells * sizeof(float4);
-    if (dyn_smem > 48 * 1024) {
-        st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
-                        "cudaFuncSetAttribute");
-        if (st != kOk) return st;
+    if (fold) {
+        FoldKernelArgs fa;
+        fa.s = a;
+        fa.xpc = xpc;
+        fa.yrows = yrows;
+        fa.plane = plane;
+        FoldKernel k = fold_y ? pick_fold<4, 2>(amp) : pick_fold<8, 1>(amp);
+        if (dyn_smem > 48 * 1024) {
+            st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
+                            "cudaFuncSetAttribute");
+            if (st != kOk) return st;
+        }
+        timer_begin(timer, 0, req.stream);
+        k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, dyn_smem, req.stream>>>(fa);
+        count_launch();
+        timer_end(timer, 0, req.stream);
+        st = check_cuda(cudaGetLastError(), "fold_sum_kernel launch");
+    } else {
+        SumKernel k = (L == 8) ? pick<8>(req.basis, amp) : pick<1>(req.basis, amp);
+        if (dyn_smem > 48 * 1024) {
+            st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
+                            "cudaFuncSetAttribute");
+            if (st != kOk) return st;
+        }
+        timer_begin(timer, 0, req.stream);
+        k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, dyn_smem, req.stream>>>(a);
+        count_launch();
+        timer_end(timer, 0, req.stream);
+        st = check_cuda(cudaGetLastError(), "plain_sum_kernel launch");
     }
-    timer_begin(timer, 0, req.stream);
-    k<<<dim3((unsigned)blocks_f, (unsigned)splits), kThreads, dyn_smem, req.stream>>>(a);
-    count_launch();
-    timer_end(timer, 0, req.stream);
-    st = check_cuda(cudaGetLastError(), "plain_sum_kernel launch");
     if (st != kOk) return st;
 
     FinalizeArgs f;

@@ -36,16 +36,18 @@
 //   warp 0       allocates TMEM, one thread issues tcgen05.mma / commit;
 //   warps 1-4    flush TMEM (warp w reads lanes 32 (w % 4) .. +31);
 //   warps 5-16   generate operands straight into shared memory in the
-//                canonical no-swizzle K-major layout (8x16-byte core matrices;
-//                16 bytes of padding between K columns of core matrices keep
-//                the stores free of bank conflicts), by recurrences along b and
+//                128-byte swizzled K-major layout (one 128-byte row of 64 FP16
+//                per operand row and stage; the swizzle lets the tensor core
+//                read at full rate and keeps the stores free of bank
+//                conflicts), by recurrences along b and
 //                c (8 steps from an exact fixed-point start, moving away from
 //                the axis origin so Gaussian factors only shrink along a chain);
 //   warp 17      streams the per-particle constants of each stage into shared
 //                memory with cp.async.bulk (global -> own CTA, no multicast),
 //                three stages ahead.
 // Per-particle constants (fixed-point positions, unit rotations, Gaussian
-// ratios) are computed once per launch by tc_prep_kernel.
+// ratios) are computed once per launch by tc_prep_kernel into 32-particle
+// field-by-field blocks.
 //
 // Every mbarrier wait is bounded (2 s of %globaltimer); a wait that runs out
 // sets *error_flag, raises the CTA's abort flag, and all roles leave their
@@ -65,16 +67,20 @@
 namespace mv {
 
 // Per-particle constants of one group, computed once per launch by
-// tc_prep_kernel (48 bytes, three float4 loads).
-struct __align__(16) TcParticle {
-    uint32_t qx, qy, qz;  // fixed-point turns of step * position
-    float amp;            // 2^12 w / W
-    float gam;            // -pi log2(e) step^2 h^2 (GAUSSIAN_DECAYING), else 0
-    float rho2;           // exp2(2 gam): ratio of successive Gaussian step factors
-    float2 ry, rz;        // exp(-2 pi i Qy / 2^32), exp(-2 pi i Qz / 2^32), accurate
-    float pad[2];
-};
-static_assert(sizeof(TcParticle) == 48, "TcParticle layout");
+// tc_prep_kernel, in blocks of 32 particles laid out field by field (1280
+// bytes per block) so that a producer reads the constants of its particle
+// pair with conflict-free 64-bit shared-memory loads, and the loader moves one
+// whole block per pipeline stage:
+//   qx[32], qy[32], qz[32]  u32 fixed-point turns of step * position
+//   amp[32]                 2^12 w / W
+//   gam[32]                 -pi log2(e) step^2 h^2 (GAUSSIAN_DECAYING), else 0
+//   rho2[32]                exp2(2 gam): ratio of successive Gaussian step factors
+//   ry[32], rz[32]          float2 exp(-2 pi i Q / 2^32), accurate
+// Particles past the group's end (up to the block boundary) have amp = 0.
+constexpr int kBlockParticles = 32;
+constexpr int kBlockBytes = 6 * 4 * kBlockParticles + 2 * 8 * kBlockParticles;  // 1280
+constexpr int kOffQx = 0, kOffQy = 128, kOffQz = 256, kOffAmp = 384, kOffGam = 512, kOffRho2 = 640, kOffRy = 768,
+              kOffRz = 1024;
 
 namespace {
 
@@ -84,18 +90,15 @@ constexpr int kN = 2 * kNc;
 constexpr int kKp = 32;
 constexpr int kKr = 2 * kKp;
 constexpr int kStages = 3;
-constexpr int kCoreBytes = 128;
-constexpr int kLbo = 16 * kCoreBytes + 16;          // bytes between K-adjacent core matrices
-constexpr int kOperandBytes = (kKr / 8) * kLbo;     // 8 K-columns of 16 core matrices
+constexpr int kRowBytes = 2 * kKr;                 // one operand row: 64 FP16 along K = one 128-byte swizzle row
+constexpr int kAtomBytes = 8 * kRowBytes;           // 8-row swizzle atom
+constexpr int kOperandBytes = kM * kRowBytes;       // 128 rows (A: M rows, B: N columns)
 constexpr int kStageBytes = 4 * kOperandBytes;      // A_hi, A_lo, B_hi, B_lo
-constexpr int kParticleBytes = 48;                  // sizeof(TcParticle)
-constexpr int kSlotBytes = kKp * kParticleBytes;    // particle constants of one stage
+constexpr int kSlotBytes = kBlockBytes;            // particle constants of one stage
 constexpr int kProducerWarps = 12;  // 8 warps of A units + 4 warps of B units, 2 chains each
 constexpr int kFlushWarps = 4;
 constexpr int kLoaderWarp = 1 + kFlushWarps + kProducerWarps;
 constexpr int kThreads = 32 * (kLoaderWarp + 1);
-constexpr int kProducerThreads = 32 * kProducerWarps;
-constexpr int kFlushThreads = 32 * kFlushWarps;
 constexpr uint32_t kTmemCols = 512;  // accumulator 0 | accumulator 1 | total | compensation
 constexpr uint32_t kColTotal = 2 * kN, kColComp = 3 * kN;
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
@@ -170,13 +173,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait: returns false (after flagging) if the phase does not complete
 // within kWaitLimitNs or the CTA is already aborting.
+// As mbar_try_wait, but a thread that finds the phase incomplete is suspended
+// until the phase completes or hint_ns nanoseconds pass, so waiting warps take
+// no issue slots from the producers.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+constexpr uint32_t kSuspendHintNs = 100000;  // 0.1 ms per suspension; the phase's completion wakes the thread first
+
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* error_flag,
                                           int code) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {
         if (*abort_flag) return false;
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait_suspend(bar, parity, kSuspendHintNs)) return true;
         if (global_ns() - t0 > kWaitLimitNs) {
             *abort_flag = 1;
             atomicOr(error_flag, code);
@@ -201,13 +220,24 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// Shared-memory descriptor of a K-major operand in the 128-byte swizzle layout:
+// row r of the operand is 128 bytes at (r / 8) * 1024 + (r % 8) * 128, its
+// 16-byte chunk j stored at chunk position j ^ (r % 8).  The operand starts on
+// a 1024-byte boundary; an MMA's K offset (32 bytes per 16 FP16) is added to the
+// start address, and the hardware applies the swizzle on the address bits.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     uint64_t d = 0;
     d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((kLbo >> 4) & 0x3FFF) << 16;        // leading (K) byte offset
-    d |= (uint64_t)((kCoreBytes >> 4) & 0x3FFF) << 32;  // stride (M/N) byte offset
+    d |= (uint64_t)1 << 16;                              // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((kAtomBytes >> 4) & 0x3FFF) << 32;  // stride byte offset: between 8-row atoms
     d |= (uint64_t)1 << 46;                              // descriptor version (sm_100)
-    return d;                                            // base offset 0, no swizzle
+    d |= (uint64_t)2 << 61;                              // 128-byte swizzle; base offset 0
+    return d;
+}
+
+// Byte offset of 16-byte chunk `chunk` of row `row` in a 128-byte-swizzled operand.
+__device__ __forceinline__ int sw128(int row, int chunk) {
+    return (row >> 3) * kAtomBytes + (row & 7) * kRowBytes + ((chunk ^ (row & 7)) << 4);
 }
 
 __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -306,15 +336,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     const int lane = tid & 31;
     const int flush_stages = a.flush_stages;
 
+    // the swizzled operands need a 1024-byte aligned shared-memory window
+    if (smem_u32(smem) & 1023u) {
+        if (tid == 0) atomicOr(a.error_flag, 128);
+        return;
+    }
+
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
-            mbar_init(&full[i], kProducerThreads);
+            mbar_init(&full[i], kProducerWarps);  // one arrival per producer warp
             mbar_init(&empty[i], 1);
             mbar_init(&pdata[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(&acc_full[i], 1);
-            mbar_init(&acc_empty[i], kFlushThreads);
+            mbar_init(&acc_empty[i], kFlushWarps);  // one arrival per flush warp
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
@@ -354,7 +390,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     const uint32_t d = tmem + (uint32_t)(b * kN);
 #pragma unroll
                     for (int t = 0; t < kKr / 16; ++t) {
-                        const uint32_t off = (uint32_t)(2 * t * kLbo);
+                        const uint32_t off = (uint32_t)(32 * t);
                         mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), (first && t == 0) ? 0u : 1u);
                         mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), 1u);
                         mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
@@ -373,7 +409,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;  // M row owned by this thread
         int C = 0;
-        for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+        for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
             const TcItem I = tc_item(a, it);
             const int lz_tc = I.job->lz_tc;
             double* acc = I.job->acc;
@@ -381,7 +417,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
                 const int b = k & 1;
-                if (!mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4)) break;
+                // warp-uniform outcome: the warp arrives as one below
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4))) break;
                 tc_fence_after();
                 const bool last = kk == I.n_chunks - 1;
 #pragma unroll 1
@@ -426,7 +463,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 }
                 tmem_wait_st();
                 tc_fence_before();
-                mbar_arrive(&acc_empty[b]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[b]);
             }
             C += I.n_chunks;
         }
@@ -442,10 +480,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     if (S >= kStages &&
                         !mbar_wait(&full[buf], ((S / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
                         break;
-                    const int j0 = I.kb + s * kKp;
-                    const uint32_t bytes = (uint32_t)(min(kKp, I.ke - j0) * kParticleBytes);
-                    mbar_arrive_expect_tx(&pdata[buf], bytes);
-                    bulk_copy_g2s(slots + buf * kSlotBytes, I.job->tp + j0, bytes, &pdata[buf]);
+                    const int block = I.kb / kBlockParticles + s;
+                    mbar_arrive_expect_tx(&pdata[buf], kBlockBytes);
+                    bulk_copy_g2s(slots + buf * kSlotBytes, I.job->blocks + (size_t)block * kBlockBytes, kBlockBytes,
+                                  &pdata[buf]);
                 }
             }
         }
@@ -458,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const int rc = (p >> 4) & 15;
         const int cb = (p >> 4) & 7;
         int S = 0;
-        for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
+        for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
             const TcItem I = tc_item(a, it);
             const int kx = I.job->kx, ky = I.job->ky, lz_tc = I.job->lz_tc;
             const bool gauss = I.job->gauss != 0;
@@ -470,34 +508,50 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             const int c_s = I.n_tile * kNc + cb * 8;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
                 const int buf = S % kStages;
-                if (!mbar_wait(&pdata[buf], (S / kStages) & 1, abort_flag, a.error_flag, 64)) break;
+                if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kStages) & 1, abort_flag, a.error_flag, 64)))
+                    break;
                 uint32_t pqx[2], pqy[2], pqz[2];
                 float pamp[2], pgam[2], prho2[2];
                 float2 pry[2], prz[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int jj = 2 * pp + e;
-                    if (I.kb + s * kKp + jj < I.ke) {
-                        const float4* src =
-                            reinterpret_cast<const float4*>(slots + buf * kSlotBytes + jj * kParticleBytes);
-                        const float4 v0 = src[0], v1 = src[1], v2 = src[2];
-                        pqx[e] = __float_as_uint(v0.x);
-                        pqy[e] = __float_as_uint(v0.y);
-                        pqz[e] = __float_as_uint(v0.z);
-                        pamp[e] = v0.w;
-                        pgam[e] = v1.x;
-                        prho2[e] = v1.y;
-                        pry[e] = make_float2(v1.z, v1.w);
-                        prz[e] = make_float2(v2.x, v2.y);
+                {
+                    // the pair's constants: particles 2pp, 2pp+1 of the stage's block
+                    const uint8_t* blk = slots + buf * kSlotBytes;
+                    const uint2 gq = *reinterpret_cast<const uint2*>(blk + kOffGam + 8 * pp);
+                    const uint2 rq = *reinterpret_cast<const uint2*>(blk + kOffRho2 + 8 * pp);
+                    pgam[0] = __uint_as_float(gq.x);
+                    pgam[1] = __uint_as_float(gq.y);
+                    prho2[0] = __uint_as_float(rq.x);
+                    prho2[1] = __uint_as_float(rq.y);
+                    if (has_a) {
+                        const uint2 x = *reinterpret_cast<const uint2*>(blk + kOffQx + 8 * pp);
+                        const uint2 y = *reinterpret_cast<const uint2*>(blk + kOffQy + 8 * pp);
+                        const uint2 w = *reinterpret_cast<const uint2*>(blk + kOffAmp + 8 * pp);
+                        const float4 r = *reinterpret_cast<const float4*>(blk + kOffRy + 16 * pp);
+                        pqx[0] = x.x;
+                        pqx[1] = x.y;
+                        pqy[0] = y.x;
+                        pqy[1] = y.y;
+                        pamp[0] = __uint_as_float(w.x);
+                        pamp[1] = __uint_as_float(w.y);
+                        pry[0] = make_float2(r.x, r.y);
+                        pry[1] = make_float2(r.z, r.w);
+                        pqz[0] = pqz[1] = 0u;
+                        prz[0] = prz[1] = make_float2(1.f, 0.f);
                     } else {
-                        pqx[e] = pqy[e] = pqz[e] = 0u;
-                        pamp[e] = 0.f;
-                        pgam[e] = 0.f;
-                        prho2[e] = 1.f;
-                        pry[e] = prz[e] = make_float2(1.f, 0.f);
+                        const uint2 zq = *reinterpret_cast<const uint2*>(blk + kOffQz + 8 * pp);
+                        const float4 r = *reinterpret_cast<const float4*>(blk + kOffRz + 16 * pp);
+                        pqz[0] = zq.x;
+                        pqz[1] = zq.y;
+                        prz[0] = make_float2(r.x, r.y);
+                        prz[1] = make_float2(r.z, r.w);
+                        pqx[0] = pqx[1] = pqy[0] = pqy[1] = 0u;
+                        pamp[0] = pamp[1] = 0.f;
+                        pry[0] = pry[1] = make_float2(1.f, 0.f);
                     }
                 }
-                if (!mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)) break;
+                if (!__all_sync(0xffffffffu,
+                                mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)))
+                    break;
                 uint8_t* st = smem + buf * kStageBytes;
                 float2 z[2], R[2];
                 float q[2], rq[2];
@@ -521,14 +575,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     }
                     uint8_t* ahi = st;
                     uint8_t* alo = st + kOperandBytes;
-                    const int col = (pp >> 1) * kLbo + rc * kCoreBytes + (pp & 1) * 8;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
                         const int r = a_up ? i : 7 - i;
+                        const int off = sw128(rc * 8 + r, pp >> 1) + (pp & 1) * 8;
                         uint2 lo;
                         const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                        *reinterpret_cast<uint2*>(ahi + col + r * 16) = hi;
-                        *reinterpret_cast<uint2*>(alo + col + r * 16) = lo;
+                        *reinterpret_cast<uint2*>(ahi + off) = hi;
+                        *reinterpret_cast<uint2*>(alo + off) = lo;
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
                             const float rx = R[e].x * q[e], ry = R[e].y * q[e];
@@ -559,13 +613,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     }
                     uint8_t* bhi = st + 2 * kOperandBytes;
                     uint8_t* blo = st + 3 * kOperandBytes;
-                    const int kcol = (pp >> 1) * kLbo + (pp & 1) * 8;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
                         uint2 lo;
                         const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                        const int re_off = kcol + cb * kCoreBytes + i * 16;
-                        const int im_off = kcol + (8 + cb) * kCoreBytes + i * 16;
+                        const int re_off = sw128(cb * 8 + i, pp >> 1) + (pp & 1) * 8;
+                        const int im_off = sw128(kNc + cb * 8 + i, pp >> 1) + (pp & 1) * 8;
                         *reinterpret_cast<uint2*>(bhi + re_off) =
                             make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
                         *reinterpret_cast<uint2*>(blo + re_off) =
@@ -584,8 +637,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         }
                     }
                 }
+                // each thread makes its stores visible to the tensor core; the
+                // warp's lane 0 then arrives for the whole warp
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(&full[buf]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&full[buf]);
             }
         }
     }
@@ -619,29 +675,36 @@ struct TcPrepArgs {
     float gamma_scale;
     float inv_wmax;
     bool gauss;
-    TcParticle* out;
+    uint8_t* out;  // ceil(n / 32) blocks
 };
 
 __global__ void tc_prep_kernel(TcPrepArgs p) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= p.n) return;
-    const float4 q = p.particles[j];
-    TcParticle t;
-    t.qx = fixed_turns(p.step * (double)q.x);
-    t.qy = fixed_turns(p.step * (double)q.y);
-    t.qz = fixed_turns(p.step * (double)q.z);
-    t.amp = q.w * p.inv_wmax * kOperandScale;
-    if (p.gauss) {
-        const float h = p.radii[j];
-        t.gam = p.gamma_scale * h * h;
-    } else {
-        t.gam = 0.f;
+    const int padded = (p.n + kBlockParticles - 1) / kBlockParticles * kBlockParticles;
+    if (j >= padded) return;
+    uint8_t* blk = p.out + (size_t)(j / kBlockParticles) * kBlockBytes;
+    const int l = j % kBlockParticles;
+    uint32_t qx = 0, qy = 0, qz = 0;
+    float amp = 0.f, gam = 0.f;
+    if (j < p.n) {
+        const float4 q = p.particles[j];
+        qx = fixed_turns(p.step * (double)q.x);
+        qy = fixed_turns(p.step * (double)q.y);
+        qz = fixed_turns(p.step * (double)q.z);
+        amp = q.w * p.inv_wmax * kOperandScale;
+        if (p.gauss) {
+            const float h = p.radii[j];
+            gam = p.gamma_scale * h * h;
+        }
     }
-    t.rho2 = exp2f(2.f * t.gam);
-    t.ry = unit_phase(t.qy);
-    t.rz = unit_phase(t.qz);
-    t.pad[0] = t.pad[1] = 0.f;
-    p.out[j] = t;
+    reinterpret_cast<uint32_t*>(blk + kOffQx)[l] = qx;
+    reinterpret_cast<uint32_t*>(blk + kOffQy)[l] = qy;
+    reinterpret_cast<uint32_t*>(blk + kOffQz)[l] = qz;
+    reinterpret_cast<float*>(blk + kOffAmp)[l] = amp;
+    reinterpret_cast<float*>(blk + kOffGam)[l] = gam;
+    reinterpret_cast<float*>(blk + kOffRho2)[l] = exp2f(2.f * gam);
+    reinterpret_cast<float2*>(blk + kOffRy)[l] = unit_phase(qy);
+    reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(qz);
 }
 
 // acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
@@ -767,7 +830,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         }
         plan.group_class.push_back(cls);
         plan.tp_offset.push_back(plan.tp_bytes);
-        plan.tp_bytes += ((size_t)std::max(0, r.n) * sizeof(TcParticle) + 255) / 256 * 256;
+        plan.tp_bytes += (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
         if (r.n <= 0 || !(r.weight_max > 0.f)) {
             plan.job_of_group.push_back(-1);
             continue;
@@ -819,7 +882,7 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     for (size_t g = 0; g < plan.job_of_group.size(); ++g) {
         const int j = plan.job_of_group[g];
         if (j < 0) continue;
-        plan.jobs[j].tp = reinterpret_cast<const TcParticle*>(tp_base + plan.tp_offset[g]);
+        plan.jobs[j].blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.tp_offset[g]);
         plan.jobs[j].acc = reinterpret_cast<double*>(acc_base + plan.classes[plan.group_class[g]].acc_offset);
     }
     std::vector<char> meta(plan.meta_bytes, 0);
@@ -863,7 +926,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         pa.gauss = plan.jobs[j].gauss != 0;
         pa.gamma_scale = pa.gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
         pa.inv_wmax = 1.0f / r.weight_max;
-        pa.out = const_cast<TcParticle*>(plan.jobs[j].tp);
+        pa.out = const_cast<unsigned char*>(plan.jobs[j].blocks);
         tc_prep_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(pa);
         count_launch();
     }
