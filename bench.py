@@ -227,6 +227,21 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def reference_groups(groups):
+    """The groups as the reference's fourier_transform can take them: it has
+    no GAUSSIAN_DECAYING (an appended basis id it skips without work), so its
+    own GAUSSIAN, with the same per-term work (one exponential), stands in."""
+    from libmeshlessvis_b200 import meshless as M
+
+    out, note = [], ""
+    for cons, radii, basis in groups:
+        if basis == M.GAUSSIAN_DECAYING:
+            basis = M.GAUSSIAN
+            note = " (GAUSSIAN_DECAYING groups timed with the reference's GAUSSIAN, the same per-term work)"
+        out.append((cons, radii, basis))
+    return out, note
+
+
 def cpu_baseline(w, target_terms=6e9):
     """The reference's own fourier_transform (OpenMP, all host threads) on the
     workload's particles, for one slice of 2*cx*cy frequencies, cx = cy chosen
@@ -239,8 +254,10 @@ def cpu_baseline(w, target_terms=6e9):
     cx, cy = c, c
     terms = n * 2 * cx * cy
     cores = len(os.sched_getaffinity(0))
+    note = ""
     if O.ref_available():
-        R = O.RefRenderer(groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
+        ref_groups, note = reference_groups(groups)
+        R = O.RefRenderer(ref_groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
         t0 = time.perf_counter()
         R.fourier_transform()
         dt = time.perf_counter() - t0
@@ -254,7 +271,36 @@ def cpu_baseline(w, target_terms=6e9):
         kind = "port"
     return {"value": terms / dt / 1e9, "unit": "GTerms/s", "cores": cores, "kind": kind,
             "sample": f"reference fourier_transform (direct slice sum) of all {n} particles over one z-normal "
-                      f"slice of 2*{cx}*{cy}={2 * cx * cy} frequencies ({terms:.3e} terms, {dt:.2f} s)"}
+                      f"slice of 2*{cx}*{cy}={2 * cx * cy} frequencies ({terms:.3e} terms, {dt:.2f} s){note}"}
+
+
+def accuracy_check(w, spec, images, n_points=1024, n_views=2):
+    """Part of the CPU-baseline leg, with the oracle as the checker: the FP64
+    direct sum at seeded half-spectrum points (the workload's own check points
+    when it has them) against the spectrum of the timed run, and FP64 slice
+    extraction + C2R of that spectrum against the first views' images."""
+    import oracle as O
+
+    kx, ky, kz = w["grid"]
+    ijk = w.get("check_points")
+    if ijk is None:
+        prng = np.random.default_rng(1)
+        ijk = np.stack([prng.integers(-kx // 2, kx // 2, n_points), prng.integers(-ky // 2, ky // 2, n_points),
+                        prng.integers(0, kz // 2 + 1, n_points)], axis=1).astype(np.int32)
+    t0 = time.perf_counter()
+    ref = sum(O.spectrum_points(c, r, b, w["step3"], ijk) for c, r, b in w["groups"])
+    got = spec[ijk[:, 0] + kx // 2, ijk[:, 1] + ky // 2, ijk[:, 2]]
+    t_spec = time.perf_counter() - t0
+    scale = float(np.max(np.abs(ref))) or 1.0
+    out = {"spectrum": {"rel_l2": O.rel_l2(got, ref), "max_abs_over_max": O.max_abs(got, ref) / scale,
+                        "points": int(len(ijk)), "tolerance": 1e-5, "oracle": "FP64 direct sum",
+                        "seconds": round(t_spec, 2)}}
+    nv = min(n_views, len(w["views"]))
+    ref_img = O.render_from_spectrum(spec.astype(np.complex128), w["grid"], w["step3"], w["step"], w["cutoff"],
+                                     w["views"][:nv], w["samples"])
+    out["images"] = {"rel_l2": O.rel_l2(images[:nv], ref_img), "views": nv, "tolerance": 1e-4,
+                     "oracle": "FP64 slice interpolation + C2R of the same spectrum"}
+    return out
 
 
 def run_reference(args):
@@ -270,8 +316,10 @@ def run_reference(args):
     terms = n * 2 * cx * cy
     cores = len(os.sched_getaffinity(0))
     kind = "reference" if O.ref_available() else "port"
+    note = ""
     if kind == "reference":
-        R = O.RefRenderer(groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
+        ref_groups, note = reference_groups(groups)
+        R = O.RefRenderer(ref_groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
         fn = R.fourier_transform
     else:
         def fn():
@@ -285,7 +333,7 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     value = terms * args.steps / dt / 1e9
     sample = (f"per step: the reference's fourier_transform (OpenMP, {cores} threads) over all {n} particles of "
-              f"workload {w['name']} and one slice of {2 * cx * cy} frequencies ({terms:.3e} terms)")
+              f"workload {w['name']} and one slice of {2 * cx * cy} frequencies ({terms:.3e} terms){note}")
     line = {"impl": "reference", "metric": "GTerms/s (particle x frequency terms per second)", "value": value,
             "unit": "GTerms/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -372,6 +420,10 @@ def run_ours(args):
     cfg.enable_timing(False)
     t_max = allmax(t_ms)
     value = replica_throughput(terms, args.steps, t_max, world) / 1e9
+    check_inputs = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the timed run's outputs, for the oracle check below (outside the timed region)
+        check_inputs = (sp.to_host(cfg), d_images[:2].cpu().numpy())
     views_per_s = replica_throughput(nv, args.steps, t_max, world)
 
     peaks, peak_src = measured_peaks()
@@ -431,8 +483,10 @@ def run_ours(args):
                "wall_ms_per_step": wall * 1000 / args.steps}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    accuracy = None
+    if check_inputs is not None:
         cpu = cpu_baseline(w)
+        accuracy = accuracy_check(w, *check_inputs)
 
     sp.close()
     cfg.unregister(ds)
@@ -454,6 +508,8 @@ def run_ours(args):
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if accuracy:
+            line["accuracy"] = accuracy
         if comparison:
             line["tc_vs_plain"] = comparison
         print(json.dumps(line), flush=True)

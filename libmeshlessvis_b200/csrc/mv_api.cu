@@ -85,6 +85,56 @@ GroupStats registered_group_stats(const void* d_constraints) {
     return it == g_stats.end() ? GroupStats{} : it->second;
 }
 
+// ------------------------------------------------------ registration pool
+// Registered particle arrays come from a stream-ordered memory pool of the
+// library's own, one per device, that keeps freed blocks (release threshold
+// unlimited): a register / unregister cycle per frame then reuses device
+// memory instead of mapping and unmapping it each time, which made cudaMalloc
+// and cudaFree of the same sizes take from under 1 ms to tens of ms.
+namespace {
+std::mutex g_pool_mu;
+std::map<int, cudaMemPool_t> g_pools;
+
+int registration_pool(cudaMemPool_t* pool) {
+    int dev = 0;
+    int st = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != kOk) return st;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) {
+        *pool = it->second;
+        return kOk;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    st = check_cuda(cudaMemPoolCreate(pool, &props), "cudaMemPoolCreate");
+    if (st != kOk) return st;
+    uint64_t keep = UINT64_MAX;
+    st = check_cuda(cudaMemPoolSetAttribute(*pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    if (st != kOk) return st;
+    g_pools[dev] = *pool;
+    return kOk;
+}
+
+template <typename T>
+int registration_alloc(T** p, size_t count, cudaStream_t stream) {
+    *p = nullptr;
+    if (count == 0) return kOk;
+    cudaMemPool_t pool;
+    int st = registration_pool(&pool);
+    if (st != kOk) return st;
+    cudaError_t e = cudaMallocFromPoolAsync((void**)p, sizeof(T) * count, pool, stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return check_cuda(e, "cudaMallocFromPoolAsync");
+    }
+    return kOk;
+}
+}  // namespace
+
 // --------------------------------------------------------------- workspace
 int Workspace::reserve(size_t need) {
     if (need <= bytes) return kOk;
@@ -497,7 +547,7 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         }
         grp.d_number_of_terms = (int)padded;
         if (padded == 0) continue;
-        if (device_alloc(&grp.d_constraints, (size_t)padded) != kOk) return;
+        if (registration_alloc(&grp.d_constraints, (size_t)padded, s->stream) != kOk) return;
         cudaMemsetAsync(grp.d_constraints, 0, sizeof(Constraint) * padded, s->stream);
         cudaMemcpyAsync(grp.d_constraints, grp.h_constraints, sizeof(Constraint) * grp.number_of_terms,
                         cudaMemcpyHostToDevice, s->stream);
@@ -517,7 +567,7 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
             g_stats[grp.d_constraints] = gs;
         }
         if (grp.h_radii) {
-            if (device_alloc(&grp.d_radii, (size_t)padded) != kOk) return;
+            if (registration_alloc(&grp.d_radii, (size_t)padded, s->stream) != kOk) return;
             cudaMemsetAsync(grp.d_radii, 0, sizeof(float) * padded, s->stream);
             cudaMemcpyAsync(grp.d_radii, grp.h_radii, sizeof(float) * grp.number_of_terms, cudaMemcpyHostToDevice,
                             s->stream);
@@ -533,14 +583,16 @@ void vis_unregister_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         set_error(kInvalidValue, "vis_unregister_meshless_dataset: NULL or unknown argument");
         return;
     }
-    cudaStreamSynchronize(s->stream);
+    // as cudaFree would: no launch on any stream still reads the arrays when
+    // their blocks go back to the pool
+    cudaDeviceSynchronize();
     for (int g = 0; g < ds->number_of_groups; ++g) {
-        cudaFree(ds->groups[g].d_constraints);
         if (ds->groups[g].d_constraints) {
+            cudaFreeAsync(ds->groups[g].d_constraints, s->stream);
             std::lock_guard<std::mutex> lock(g_stats_mu);
             g_stats.erase(ds->groups[g].d_constraints);
         }
-        cudaFree(ds->groups[g].d_radii);
+        if (ds->groups[g].d_radii) cudaFreeAsync(ds->groups[g].d_radii, s->stream);
         ds->groups[g].d_constraints = nullptr;
         ds->groups[g].d_radii = nullptr;
     }
