@@ -131,7 +131,7 @@ int tensor_sum_available(const SumRequest& req);
 // + n_tile.  Device-resident (64 bytes).
 struct TcJob {
     const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
-    double* acc;           // [(a_idx * ky + b_idx) * lz_tc + c][2]
+    double* acc;           // [c][Re, Im][a_idx * ky + b_idx]
     double wmax;
     int kx, ky, lz_tc;  // lattice extents; c planes [0, lz_tc) are summed here
     int n_mtiles, n_ntiles;
@@ -153,7 +153,8 @@ struct TensorPlan {
         size_t acc_offset;
     };
     std::vector<TcJob> jobs;
-    std::vector<int2> items;
+    std::vector<int2> items;  // NMAX = 128 items first (n_narrow of them), then NMAX = 256
+    int n_narrow = 0;
     std::vector<Class> classes;
     std::vector<int> group_class, job_of_group;
     std::vector<size_t> tp_offset;

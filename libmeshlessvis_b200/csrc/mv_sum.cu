@@ -234,7 +234,9 @@ __global__ void __launch_bounds__(kThreads, 2) plain_sum_kernel(SumKernelArgs a)
 // (and (+-xp, -yp)) together: one amplitude evaluation and one x rotation
 // serve up to four lattice points.  With u = amp c, the four real sums
 //   A0 = sum ur dr, A1 = sum ui di, A2 = sum ur di, A3 = sum ui dr
-// give T(+xp) = (A0 - A1, A2 + A3) and T(-xp) = (A0 + A1, A2 - A3).
+// give T(+xp) = (A0 - A1, A2 + A3) and T(-xp) = (A0 + A1, A2 - A3); they are
+// kept as the pairs (A0, A3) += u (dr, dr) and (A2, A1) += u (di, di), one
+// packed FP32 FMA (sm_100 FFMA2) each.
 // Terms outside the lattice and the mirrors of xp = 0 / yp = 0 are computed
 // but not stored.  The partial-sum layout is the plain kernel's.
 struct FoldKernelArgs {
@@ -279,12 +281,12 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
         }
     }
 
-    constexpr int NS = 4 * FY;  // real sums per representative
-    float tot[L][NS], comp[L][NS];
+    constexpr int NP = 2 * FY;  // packed pairs of real sums per representative
+    float2 tot[L][NP], comp[L][NP];
 #pragma unroll
     for (int m = 0; m < L; ++m)
 #pragma unroll
-        for (int i = 0; i < NS; ++i) tot[m][i] = comp[m][i] = 0.f;
+        for (int i = 0; i < NP; ++i) tot[m][i] = comp[m][i] = make_float2(0.f, 0.f);
 
     const int beg = blockIdx.y * a.chunk;
     const int end = min(a.n, beg + a.chunk);
@@ -312,11 +314,11 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
         __syncthreads();
         const int cnt = min(kThreads, end - t0);
 
-        float acc[L][NS];
+        float2 acc[L][NP];
 #pragma unroll
         for (int m = 0; m < L; ++m)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) acc[m][i] = 0.f;
+            for (int i = 0; i < NP; ++i) acc[m][i] = make_float2(0.f, 0.f);
 
 #pragma unroll 1
         for (int j = 0; j < cnt; ++j) {
@@ -328,12 +330,12 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
             const uint32_t pyz = uy * q.y + uz * q.z;
             float sn, cs;
             __sincosf(turns_to_radians(pyz), &sn, &cs);
-            const float dpr = w * cs, dpi = w * sn;
-            float dmr = 0.f, dmi = 0.f;
+            const float2 dpr = make_float2(w * cs, w * cs), dpi = make_float2(w * sn, w * sn);
+            float2 dmr = make_float2(0.f, 0.f), dmi = make_float2(0.f, 0.f);
             if constexpr (FY == 2) {
                 __sincosf(turns_to_radians(pyz - 2u * uy * q.y), &sn, &cs);
-                dmr = w * cs;
-                dmi = w * sn;
+                dmr = make_float2(w * cs, w * cs);
+                dmi = make_float2(w * sn, w * sn);
             }
             __sincosf(turns_to_radians(uxb * q.x), &sn, &cs);
             float cr = cs, ci = sn;
@@ -343,10 +345,12 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
                 if constexpr (AMP != kAmpFactored) {
                     float amp;
                     if constexpr (AMP == kAmpTable) {
-                        const float u = r[m] * hv;  // s / ds
-                        const float tt = u + 12582912.0f;  // round to nearest cell (1.5 * 2^23)
+                        // s / ds = r hv: nearest cell and offset (1.5 * 2^23 rounds)
+                        const float tt = fmaf(r[m], hv, 12582912.0f);
+                        const float fr = fmaf(r[m], hv, -(tt - 12582912.0f));
+                        // beyond the table (and for negative radii) the last,
+                        // all-zero cell is used
                         const unsigned k = min((unsigned)(__float_as_int(tt) - 0x4B400000), (unsigned)a.table_n);
-                        const float fr = u - (tt - 12582912.0f);
                         const float4 c = s_tab[k];
                         amp = fmaf(fmaf(fmaf(c.w, fr, c.z), fr, c.y), fr, c.x);
                     } else {
@@ -355,15 +359,12 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
                     ur *= amp;
                     ui *= amp;
                 }
-                acc[m][0] = fmaf(ur, dpr, acc[m][0]);
-                acc[m][1] = fmaf(ui, dpi, acc[m][1]);
-                acc[m][2] = fmaf(ur, dpi, acc[m][2]);
-                acc[m][3] = fmaf(ui, dpr, acc[m][3]);
+                const float2 u = make_float2(ur, ui);
+                acc[m][0] = __ffma2_rn(u, dpr, acc[m][0]);  // (A0, A3)
+                acc[m][1] = __ffma2_rn(u, dpi, acc[m][1]);  // (A2, A1)
                 if constexpr (FY == 2) {
-                    acc[m][4] = fmaf(ur, dmr, acc[m][4]);
-                    acc[m][5] = fmaf(ui, dmi, acc[m][5]);
-                    acc[m][6] = fmaf(ur, dmi, acc[m][6]);
-                    acc[m][7] = fmaf(ui, dmr, acc[m][7]);
+                    acc[m][2] = __ffma2_rn(u, dmr, acc[m][2]);
+                    acc[m][3] = __ffma2_rn(u, dmi, acc[m][3]);
                 }
                 if (m + 1 < L) {
                     const float nr = fmaf(cr, R.x, -ci * R.y);
@@ -377,10 +378,11 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
 #pragma unroll
         for (int m = 0; m < L; ++m)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) {
-                const float yv = acc[m][i] - comp[m][i];
-                const float tv = tot[m][i] + yv;
-                comp[m][i] = (tv - tot[m][i]) - yv;
+            for (int i = 0; i < NP; ++i) {
+                const float2 yv = __fadd2_rn(acc[m][i], make_float2(-comp[m][i].x, -comp[m][i].y));
+                const float2 tv = __fadd2_rn(tot[m][i], yv);
+                const float2 dt = __fadd2_rn(tv, make_float2(-tot[m][i].x, -tot[m][i].y));
+                comp[m][i] = __fadd2_rn(dt, make_float2(-yv.x, -yv.y));
                 tot[m][i] = tv;
             }
     }
@@ -391,20 +393,20 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
     const int y_lo = a.lat.y0, y_hi = a.lat.y0 + a.lat.ny - 1;
 #pragma unroll
     for (int m = 0; m < L; ++m) {
-        float v[NS];
-#pragma unroll
-        for (int i = 0; i < NS; ++i) v[i] = tot[m][i] - comp[m][i];
         const int xp = xb + m;
 #pragma unroll
         for (int sy = 0; sy < FY; ++sy) {
             const int y = sy == 0 ? yp : -yp;
             if (sy == 1 && yp == 0) continue;
             if (y < y_lo || y > y_hi) continue;
-            const float* A = v + 4 * sy;
+            // (A0, A3) and (A2, A1) of this y sign
+            const float2 p0 = make_float2(tot[m][2 * sy].x - comp[m][2 * sy].x, tot[m][2 * sy].y - comp[m][2 * sy].y);
+            const float2 p1 =
+                make_float2(tot[m][2 * sy + 1].x - comp[m][2 * sy + 1].x, tot[m][2 * sy + 1].y - comp[m][2 * sy + 1].y);
             const size_t rest = (size_t)(y - y_lo) * nz + (z - a.lat.z0);
-            if (xp <= x_hi) out[(size_t)(xp - x_lo) * a.n_rest + rest] = make_float2(A[0] - A[1], A[2] + A[3]);
+            if (xp <= x_hi) out[(size_t)(xp - x_lo) * a.n_rest + rest] = make_float2(p0.x - p1.y, p1.x + p0.y);
             if (xp > 0 && -xp >= x_lo)
-                out[(size_t)(-xp - x_lo) * a.n_rest + rest] = make_float2(A[0] + A[1], A[2] - A[3]);
+                out[(size_t)(-xp - x_lo) * a.n_rest + rest] = make_float2(p0.x + p1.y, p1.x - p0.y);
         }
     }
 }

@@ -21,21 +21,25 @@
 // x 2^12 = hi + lo with hi, lo FP16; the scale keeps lo a normal FP16 number
 // for every |x| >= 2^-15 (below that the absolute error is < 2^-36).  The three
 // products hi*hi + hi*lo + lo*hi (error ~2^-22 relative) accumulate into ONE
-// TMEM accumulator (FP32, units of 2^24).  Two accumulators alternate: while the
-// MMAs fill one, the flush warps fold the other into a Kahan-compensated FP32
-// running total also kept in TMEM.  This bounds every tensor-core accumulation
-// chain to flush_stages x 12 MMAs (the tensor core's FP32 accumulation loses
-// accuracy with chain length: 1.2e-6 rel-L2 at 4 stages, 5.2e-6 at 64).  At
-// the end of the particle range the total is added to an FP64 accumulator in
-// global memory (one RED.ADD.F64 per frequency and work item), which a
-// finalize kernel converts to the float2 spectrum.
+// TMEM accumulator (FP32, units of 2^24; 256 columns).  Every flush_stages
+// stages (a chain of flush_stages x 12 MMAs; the tensor core's FP32
+// accumulation loses accuracy with chain length: 1.6e-6 rel-L2 at 4 stages,
+// 2.4e-6 at 8, 4.1e-6 at 16) the MMA pauses while the flush warps add the
+// accumulator into an FP32 total in the other 256 TMEM columns.  Every
+// kDumpFlushes chains, and at the end of the particle range, the total goes
+// to an FP64 accumulator in global memory (RED.ADD.F64, laid out [c][Re, Im][row]
+// so a warp's rows are contiguous), which a finalize kernel converts to the
+// float2 spectrum.
 //
-// CTA tile: M = 128 rows (a, b) (8-row chunks of constant a), N = 64 c values
-// (128 real columns), K = 32 particles (64 real) per pipeline stage, 3 stages.
+// CTA tile: M = 128 rows (a, b) (8-row chunks of constant a), N = up to 128 c
+// values (256 real columns: the 128x256 MMA reads A once for twice the work of
+// a 128x128 one, within the shared-memory port), K = 32 particles (64 real)
+// per pipeline stage, 2 stages.
 // Warp roles:
 //   warp 0       allocates TMEM, one thread issues tcgen05.mma / commit;
 //   warps 1-4    flush TMEM (warp w reads lanes 32 (w % 4) .. +31);
-//   warps 5-16   generate operands straight into shared memory in the
+//   warps 5-16   generate operands straight into shared memory (8 warps of A
+//                row chunks, 4 of B c chunks, two chunks per thread) in the
 //                128-byte swizzled K-major layout (one 128-byte row of 64 FP16
 //                per operand row and stage; the swizzle lets the tensor core
 //                read at full rate and keeps the stores free of bank
@@ -44,7 +48,7 @@
 //                the axis origin so Gaussian factors only shrink along a chain);
 //   warp 17      streams the per-particle constants of each stage into shared
 //                memory with cp.async.bulk (global -> own CTA, no multicast),
-//                three stages ahead.
+//                two stages ahead.
 // Per-particle constants (fixed-point positions, unit rotations, Gaussian
 // ratios) are computed once per launch by tc_prep_kernel into 32-particle
 // field-by-field blocks.
@@ -85,30 +89,49 @@ constexpr int kOffQx = 0, kOffQy = 128, kOffQz = 256, kOffAmp = 384, kOffGam = 5
 namespace {
 
 constexpr int kM = 128;
-constexpr int kNc = 64;
-constexpr int kN = 2 * kNc;
 constexpr int kKp = 32;
 constexpr int kKr = 2 * kKp;
-constexpr int kStages = 3;
 constexpr int kRowBytes = 2 * kKr;                 // one operand row: 64 FP16 along K = one 128-byte swizzle row
 constexpr int kAtomBytes = 8 * kRowBytes;           // 8-row swizzle atom
-constexpr int kOperandBytes = kM * kRowBytes;       // 128 rows (A: M rows, B: N columns)
-constexpr int kStageBytes = 4 * kOperandBytes;      // A_hi, A_lo, B_hi, B_lo
+constexpr int kABytes = kM * kRowBytes;             // A operand: 128 rows
 constexpr int kSlotBytes = kBlockBytes;            // particle constants of one stage
-constexpr int kProducerWarps = 12;  // 8 warps of A units + 4 warps of B units, 2 chains each
+constexpr int kProducerWarps = 12;  // 8 warps of A units + 4 warps of B units
 constexpr int kFlushWarps = 4;
 constexpr int kLoaderWarp = 1 + kFlushWarps + kProducerWarps;
 constexpr int kThreads = 32 * (kLoaderWarp + 1);
-constexpr uint32_t kTmemCols = 512;  // accumulator 0 | accumulator 1 | total | compensation
-constexpr uint32_t kColTotal = 2 * kN, kColComp = 3 * kN;
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kColTotal = 256;  // FP32 total: columns [256, 256 + NMAX)
+constexpr int kDumpFlushes = 16;  // chain partials summed in FP32 before an FP64 dump
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
 constexpr float kInvProductScale = 1.f / (4096.f * 4096.f);  // 2^-24
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
-constexpr size_t kBarrierOffset = (size_t)kStages * (kStageBytes + kSlotBytes);
-constexpr size_t kSmemBytes = kBarrierOffset + 256;
 
-// idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, N = 128, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+// The two tile widths.  NMAX = real accumulator columns of an n-tile (Re | Im
+// of NMAX / 2 c values):
+//   NMAX = 128: two 128-column TMEM accumulators alternate, so the MMAs never
+//               wait for a flush; 3 stages of 64 KB operands;
+//   NMAX = 256: one 256-column accumulator (the MMA waits while a flush reads
+//               it); 2 stages of 96 KB.  The 128x256 MMA reads A once for
+//               twice the work of a 128x128 one, which keeps its operand reads
+//               within the shared-memory port.
+// A job takes NMAX = 128 when its lattice has at most 64 tensor planes.
+template <int NMAX>
+struct Shape {
+    static constexpr int kNc = NMAX / 2;                      // c values per n-tile
+    static constexpr int kStages = NMAX == 128 ? 3 : 2;
+    static constexpr int kBufs = NMAX == 128 ? 2 : 1;         // TMEM accumulators, NMAX columns each
+    static constexpr int kBBytes = NMAX * kRowBytes;          // B operand: NMAX rows
+    static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
+    static constexpr int kChunksPerThread = NMAX / 128;       // 8-c chunks per B producer thread
+    static constexpr size_t kBarrierOffset = (size_t)kStages * (kStageBytes + kSlotBytes);
+    static constexpr size_t kSmemBytes = kBarrierOffset + 256;
+};
+static_assert(Shape<256>::kSmemBytes <= 227 * 1024 && Shape<128>::kSmemBytes <= 227 * 1024, "shared memory");
+
+// idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t mma_idesc(int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+}
 
 
 struct TcArgs {
@@ -125,8 +148,10 @@ struct TcItem {
     int m_tile, n_tile;
     int kb, ke;
     int n_stages, n_chunks;
+    int nc;  // c values of this n-tile (a multiple of 8); the MMA's N is 2 nc
 };
 
+template <int NMAX>
 __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
     const int2 v = a.items[it];
     TcItem r;
@@ -140,6 +165,7 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
     r.ke = min(r.job->n, r.kb + r.job->k_chunk);
     r.n_stages = max(0, (r.ke - r.kb + kKp - 1) / kKp);
     r.n_chunks = (r.n_stages + a.flush_stages - 1) / a.flush_stages;
+    r.nc = min(Shape<NMAX>::kNc, r.job->lz_tc - r.n_tile * Shape<NMAX>::kNc);
     return r;
 }
 
@@ -240,12 +266,13 @@ __device__ __forceinline__ int sw128(int row, int chunk) {
     return (row >> 3) * kAtomBytes + (row & 7) * kRowBytes + ((chunk ^ (row & 7)) << 4);
 }
 
-__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 
@@ -318,15 +345,18 @@ __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_secon
 // pipeline's stage and chunk counters (hence mbarrier phases and the TMEM
 // accumulator parity) run on across items; TMEM and the barriers are set up
 // once per CTA.
+template <int NMAX>
 __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
+    using SH = Shape<NMAX>;
+    constexpr int kStages = SH::kStages, kStageBytes = SH::kStageBytes, kBufs = SH::kBufs;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* slots = smem + kStages * kStageBytes;  // [kStages][kSlotBytes]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kBarrierOffset);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SH::kBarrierOffset);
     uint64_t* full = bars;                   // [kStages] producers -> MMA
     uint64_t* empty = bars + kStages;        // [kStages] MMA -> producers
     uint64_t* pdata = bars + 2 * kStages;    // [kStages] loader -> producers
-    uint64_t* acc_full = bars + 3 * kStages;   // [2] MMA -> flush
-    uint64_t* acc_empty = acc_full + 2;         // [2] flush -> MMA
+    uint64_t* acc_full = bars + 3 * kStages;   // [kBufs] MMA -> flush: a chain is complete
+    uint64_t* acc_empty = acc_full + 2;         // [kBufs] flush -> MMA: the accumulator has been read
     uint64_t* drain = acc_full + 4;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(acc_full + 5);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(acc_full + 5) + 1;
@@ -348,7 +378,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             mbar_init(&empty[i], 1);
             mbar_init(&pdata[i], 1);
         }
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kBufs; ++i) {
             mbar_init(&acc_full[i], 1);
             mbar_init(&acc_empty[i], kFlushWarps);  // one arrival per flush warp
         }
@@ -371,29 +401,29 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     if (warp == 0) {
         // ------------------------------------------------------------- MMA
         if (lane == 0) {
-            int S = 0, C = 0;  // stages and chunks issued so far by this CTA
+            int S = 0, C = 0;  // stages and chains issued so far by this CTA
             for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
-                const TcItem I = tc_item(a, it);
+                const TcItem I = tc_item<NMAX>(a, it);
+                const uint32_t idesc = mma_idesc(2 * I.nc);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
                     const int buf = S % kStages;
-                    const int k = C + s / flush_stages;
-                    const int b = k & 1;
+                    const int k = C + s / flush_stages;  // chain index
+                    const int b = k % kBufs, u = k / kBufs;  // accumulator and its use count
                     const bool first = (s % flush_stages) == 0;
-                    if (first && k >= 2 &&
-                        !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1, abort_flag, a.error_flag, 1))
-                        break;
+                    // a chain starts once the flush of the accumulator's previous chain has read it
+                    if (first && u >= 1 && !mbar_wait(&acc_empty[b], (u - 1) & 1, abort_flag, a.error_flag, 1)) break;
                     if (!mbar_wait(&full[buf], (S / kStages) & 1, abort_flag, a.error_flag, 2)) break;
                     tc_fence_after();
                     const uint32_t base = smem_u32(smem + buf * kStageBytes);
-                    const uint32_t a_hi = base, a_lo = base + kOperandBytes;
-                    const uint32_t b_hi = base + 2 * kOperandBytes, b_lo = base + 3 * kOperandBytes;
-                    const uint32_t d = tmem + (uint32_t)(b * kN);
+                    const uint32_t a_hi = base, a_lo = base + kABytes;
+                    const uint32_t b_hi = base + 2 * kABytes, b_lo = b_hi + SH::kBBytes;
+                    const uint32_t d = tmem + (uint32_t)(b * NMAX);
 #pragma unroll
                     for (int t = 0; t < kKr / 16; ++t) {
                         const uint32_t off = (uint32_t)(32 * t);
-                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), (first && t == 0) ? 0u : 1u);
-                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), 1u);
-                        mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), 1u);
+                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc, (first && t == 0) ? 0u : 1u);
+                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
+                        mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, 1u);
                     }
                     mma_commit(&empty[buf]);
                     if ((s % flush_stages) == flush_stages - 1 || s == I.n_stages - 1) mma_commit(&acc_full[b]);
@@ -410,70 +440,62 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const int row = quarter * 32 + lane;  // M row owned by this thread
         int C = 0;
         for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
-            const TcItem I = tc_item(a, it);
-            const int lz_tc = I.job->lz_tc;
+            const TcItem I = tc_item<NMAX>(a, it);
+            const size_t mk = (size_t)I.job->kx * I.job->ky;
             double* acc = I.job->acc;
             const double wmax = I.job->wmax;
+            const int rho = I.m_tile * kM + row;
+            const int c0 = I.n_tile * SH::kNc;
+            const int ncols = 2 * I.nc;
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
-                const int b = k & 1;
+                const int b = k % kBufs, u = k / kBufs;
+                const uint32_t acc_col = lane_base + (uint32_t)(b * NMAX);
                 // warp-uniform outcome: the warp arrives as one below
-                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (k >> 1) & 1, abort_flag, a.error_flag, 4))) break;
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, 4))) break;
                 tc_fence_after();
-                const bool last = kk == I.n_chunks - 1;
+                tmem_wait_st();  // the previous flush's stores of the total
+                // chain partials are summed in FP32 for kDumpFlushes chains, then
+                // dumped into the FP64 accumulator (and at the item's end)
+                const bool first = (kk % kDumpFlushes) == 0;
+                const bool dump = (kk % kDumpFlushes) == kDumpFlushes - 1 || kk == I.n_chunks - 1;
 #pragma unroll 1
-                for (int cc = 0; cc < kN / 16; ++cc) {
-                    float dv[16], tt[16], cp[16];
-                    tmem_ld16(lane_base + b * kN + cc * 16, dv);
-                    if (kk > 0) {
-                        tmem_ld16(lane_base + kColTotal + cc * 16, tt);
-                        tmem_ld16(lane_base + kColComp + cc * 16, cp);
-                    }
+                for (int cc = 0; cc < ncols / 16; ++cc) {
+                    float dv[16], tt[16];
+                    tmem_ld16(acc_col + cc * 16, dv);
+                    if (!first) tmem_ld16(lane_base + kColTotal + cc * 16, tt);
                     tmem_wait_ld();
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const float v = dv[i] * kInvProductScale;
-                        if (kk == 0) {
-                            tt[i] = v;
-                            cp[i] = 0.f;
-                        } else {
-                            const float y = v - cp[i];
-                            const float t = tt[i] + y;
-                            cp[i] = (t - tt[i]) - y;
-                            tt[i] = t;
-                        }
+                        tt[i] = first ? v : tt[i] + v;
                     }
-                    if (!last) {
+                    if (!dump) {
                         tmem_st16(lane_base + kColTotal + cc * 16, tt);
-                        tmem_st16(lane_base + kColComp + cc * 16, cp);
                     } else {
-                        // add the item's total to the FP64 accumulator
-                        const int rho = I.m_tile * kM + row;
-                        const int c0 = I.n_tile * kNc;
+                        // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are contiguous
 #pragma unroll
                         for (int i = 0; i < 16; ++i) {
                             const int n = cc * 16 + i;
-                            const int c = c0 + (n % kNc);
-                            if (c < lz_tc) {
-                                const double v = ((double)tt[i] - (double)cp[i]) * wmax;
-                                atomicAdd(acc + ((size_t)rho * lz_tc + c) * 2 + (n / kNc), v);
-                            }
+                            const int im = n >= I.nc ? 1 : 0;
+                            const int c = c0 + n - im * I.nc;
+                            atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * wmax);
                         }
                     }
                 }
-                tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&acc_empty[b]);
             }
             C += I.n_chunks;
         }
+        tmem_wait_st();  // nothing in flight when TMEM is released (abort path)
     } else if (warp == kLoaderWarp) {
         // ---------------------------------------------------------- loader
         if (lane == 0) {
             int S = 0;
             for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
-                const TcItem I = tc_item(a, it);
+                const TcItem I = tc_item<NMAX>(a, it);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
                     const int buf = S % kStages;
                     // the producers are done with this slot once stage S - kStages is full
@@ -492,20 +514,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         // -------------------------------------------------------- producers
         const int p = tid - 32 * (1 + kFlushWarps);
         const int pp = p & 15;  // particle pair within the stage
-        const bool has_a = p < 256;  // A unit: 8-row chunk rc; else B unit: 8-column chunk cb
+        const bool has_a = p < 256;  // A unit: 8-row chunk rc; else B unit: c chunks cb, cb + 8
         const int rc = (p >> 4) & 15;
         const int cb = (p >> 4) & 7;
         int S = 0;
         for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
-            const TcItem I = tc_item(a, it);
-            const int kx = I.job->kx, ky = I.job->ky, lz_tc = I.job->lz_tc;
+            const TcItem I = tc_item<NMAX>(a, it);
+            const int kx = I.job->kx, ky = I.job->ky;
             const bool gauss = I.job->gauss != 0;
             const int rho0 = I.m_tile * kM + rc * 8;
             const int a_x = rho0 / ky - kx / 2;
             const int b0 = rho0 % ky - ky / 2;
             const bool a_up = b0 >= 0;
             const int b_s = a_up ? b0 : b0 + 7;
-            const int c_s = I.n_tile * kNc + cb * 8;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
                 const int buf = S % kStages;
                 if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kStages) & 1, abort_flag, a.error_flag, 64)))
@@ -574,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         z[e] = make_float2(g * cs, -g * sn);
                     }
                     uint8_t* ahi = st;
-                    uint8_t* alo = st + kOperandBytes;
+                    uint8_t* alo = st + kABytes;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
                         const int r = a_up ? i : 7 - i;
@@ -593,47 +614,55 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         }
                     }
                 } else {
-                    // ---- B: columns cb*8 .. cb*8+7 (Re) and 64 + ... (Im), scaled by 2^12
-                    const bool live = c_s < lz_tc;
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        float sn, cs;
-                        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
-                        float g = live ? kOperandScale : 0.f;
-                        R[e] = prz[e];
-                        if (gauss) {
-                            g *= exp2f(pgam[e] * (float)(c_s * c_s));
-                            q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
-                            rq[e] = prho2[e];
-                        } else {
-                            q[e] = 1.f;
-                            rq[e] = 1.f;
-                        }
-                        z[e] = make_float2(g * cs, -g * sn);
-                    }
-                    uint8_t* bhi = st + 2 * kOperandBytes;
-                    uint8_t* blo = st + 3 * kOperandBytes;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        uint2 lo;
-                        const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                        const int re_off = sw128(cb * 8 + i, pp >> 1) + (pp & 1) * 8;
-                        const int im_off = sw128(kNc + cb * 8 + i, pp >> 1) + (pp & 1) * 8;
-                        *reinterpret_cast<uint2*>(bhi + re_off) =
-                            make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
-                        *reinterpret_cast<uint2*>(blo + re_off) =
-                            make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
-                        *reinterpret_cast<uint2*>(bhi + im_off) =
-                            make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
-                        *reinterpret_cast<uint2*>(blo + im_off) =
-                            make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
+                    // ---- B: c chunks cb and cb + 8 of the n-tile (8 c values each),
+                    // scaled by 2^12; rows [0, nc) hold (Re B, -Im B) pairs (the
+                    // Re F columns), rows [nc, 2 nc) (Im B, Re B) (the Im F columns).
+                    // Chunks at or beyond nc are not read by the MMA (N = 2 nc).
+                    uint8_t* bhi = st + 2 * kABytes;
+                    uint8_t* blo = bhi + SH::kBBytes;
+#pragma unroll 1
+                    for (int h = 0; h < SH::kChunksPerThread; ++h) {
+                        const int chunk = cb + 8 * h;
+                        if (chunk * 8 >= I.nc) break;
+                        const int c_s = I.n_tile * SH::kNc + chunk * 8;
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
-                            const float rx = R[e].x * q[e], ry = R[e].y * q[e];
-                            const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
-                            const float ny = fmaf(z[e].x, ry, z[e].y * rx);
-                            z[e] = make_float2(nx, ny);
-                            q[e] *= rq[e];
+                            float sn, cs;
+                            __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
+                            float g = kOperandScale;
+                            R[e] = prz[e];
+                            if (gauss) {
+                                g *= exp2f(pgam[e] * (float)(c_s * c_s));
+                                q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
+                                rq[e] = prho2[e];
+                            } else {
+                                q[e] = 1.f;
+                                rq[e] = 1.f;
+                            }
+                            z[e] = make_float2(g * cs, -g * sn);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            uint2 lo;
+                            const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
+                            const int re_off = sw128(chunk * 8 + i, pp >> 1) + (pp & 1) * 8;
+                            const int im_off = sw128(I.nc + chunk * 8 + i, pp >> 1) + (pp & 1) * 8;
+                            *reinterpret_cast<uint2*>(bhi + re_off) =
+                                make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
+                            *reinterpret_cast<uint2*>(blo + re_off) =
+                                make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
+                            *reinterpret_cast<uint2*>(bhi + im_off) =
+                                make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
+                            *reinterpret_cast<uint2*>(blo + im_off) =
+                                make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const float rx = R[e].x * q[e], ry = R[e].y * q[e];
+                                const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
+                                const float ny = fmaf(z[e].x, ry, z[e].y * rx);
+                                z[e] = make_float2(nx, ny);
+                                q[e] *= rq[e];
+                            }
                         }
                     }
                 }
@@ -734,7 +763,10 @@ __global__ void tc_finalize_kernel(TcFinalizeArgs f) {
         const double k = f.step * sqrt((double)a * a + (double)b * b + (double)c * c);
         factor *= phi_fp64(f.basis, k * f.h);
     }
-    const float re = (float)(f.acc[2 * q] * factor), im = (float)(f.acc[2 * q + 1] * factor);
+    // accumulator layout [c][Re, Im][row]
+    const size_t mk = (size_t)f.kx * f.ky;
+    const float re = (float)(f.acc[(size_t)(2 * c) * mk + rho] * factor);
+    const float im = (float)(f.acc[(size_t)(2 * c + 1) * mk + rho] * factor);
     const size_t idx = (size_t)rho * f.lz_out + c;
     if (f.accumulate) {
         const float2 o = f.out[idx];
@@ -798,7 +830,13 @@ struct ClassKey {
 int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     plan = TensorPlan{};
     std::vector<ClassKey> keys;
-    std::vector<std::pair<long long, int2>> items;  // (stages, item)
+    // (narrow tile?, stages, item): NMAX = 128 items first, each kind longest first
+    struct Item {
+        int wide;
+        long long cost;
+        int2 item;
+    };
+    std::vector<Item> items;
     const int flush = tc_flush_stages();
     for (size_t g = 0; g < groups.size(); ++g) {
         const SumRequest& r = groups[g];
@@ -839,8 +877,10 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.kx = kx;
         j.ky = ky;
         j.lz_tc = lz_tc;
+        const int wide = lz_tc > Shape<128>::kNc ? 1 : 0;  // NMAX = 256 beyond 64 tensor planes
+        const int nc_tile = wide ? Shape<256>::kNc : Shape<128>::kNc;
         j.n_mtiles = (int)((long long)kx * ky / kM);
-        j.n_ntiles = (lz_tc + kNc - 1) / kNc;
+        j.n_ntiles = (lz_tc + nc_tile - 1) / nc_tile;
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
@@ -860,14 +900,20 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(r.n, k0 + chunk);
             const long long stages = (k1 - k0 + kKp - 1) / kKp;
             for (long long t = 0; t < ftiles; ++t)
-                items.push_back({stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+                items.push_back({wide, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
         }
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
-    // longest first, then round-robin over the persistent CTAs
-    std::stable_sort(items.begin(), items.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    // per tile width, longest first (round-robin over the persistent CTAs)
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) {
+        return x.wide != y.wide ? x.wide < y.wide : x.cost > y.cost;
+    });
     plan.items.reserve(items.size());
-    for (auto& it : items) plan.items.push_back(it.second);
+    plan.n_narrow = 0;
+    for (auto& it : items) {
+        plan.items.push_back(it.item);
+        plan.n_narrow += it.wide ? 0 : 1;
+    }
     plan.meta_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256 + plan.items.size() * sizeof(int2);
     return kOk;
 }
@@ -932,24 +978,35 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
     }
     st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
     if (st != kOk) return st;
-    // one persistent launch for all groups
+    // one persistent launch per tile width for all groups
     if (!plan.items.empty()) {
-        TcArgs a;
-        a.jobs = static_cast<const TcJob*>(plan.d_jobs);
-        a.items = static_cast<const int2*>(plan.d_items);
-        a.n_items = (int)plan.items.size();
-        a.flush_stages = tc_flush_stages();
-        a.error_flag = error_flag;
-        st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kSmemBytes),
-                        "cudaFuncSetAttribute");
-        if (st != kOk) return st;
-        const int grid = std::min<int>(a.n_items, device_sm_count());
         timer_begin(timer, 3, stream);
-        tc_sum_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
-        count_launch();
+        for (int wide = 0; wide < 2 && st == kOk; ++wide) {
+            TcArgs a;
+            a.jobs = static_cast<const TcJob*>(plan.d_jobs);
+            a.items = static_cast<const int2*>(plan.d_items) + (wide ? plan.n_narrow : 0);
+            a.n_items = wide ? (int)plan.items.size() - plan.n_narrow : plan.n_narrow;
+            a.flush_stages = tc_flush_stages();
+            a.error_flag = error_flag;
+            if (a.n_items == 0) continue;
+            const int grid = std::min<int>(a.n_items, device_sm_count());
+            if (wide) {
+                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)Shape<256>::kSmemBytes),
+                                "cudaFuncSetAttribute");
+                if (st != kOk) break;
+                tc_sum_kernel<256><<<grid, kThreads, Shape<256>::kSmemBytes, stream>>>(a);
+            } else {
+                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)Shape<128>::kSmemBytes),
+                                "cudaFuncSetAttribute");
+                if (st != kOk) break;
+                tc_sum_kernel<128><<<grid, kThreads, Shape<128>::kSmemBytes, stream>>>(a);
+            }
+            count_launch();
+            st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");
+        }
         timer_end(timer, 3, stream);
-        st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");
         if (st != kOk) return st;
     }
     // FP64 accumulators -> spectra (added to what is there)

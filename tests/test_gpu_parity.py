@@ -261,6 +261,19 @@ def test_tensor_form_matches_fp64(case):
     assert O.rel_l2(imgs, ref_imgs) < IMAGE_TOL
 
 
+@pytest.mark.parametrize("case", ["gauss_decaying_radii", "wendland_uniform_radius"])
+def test_tensor_form_two_n_tiles_of_unequal_width(case):
+    """A 32x32x272 lattice: the tensor planes c < 136 split into an n-tile of
+    128 c values (MMA N = 256) and one of 8 (N = 16, the smallest MMA width)."""
+    rng = np.random.default_rng(23)
+    groups = _tc_groups(rng, 2001)[case]
+    grid = (32, 32, 272)
+    spec, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+    ref = O.spectrum_grid(groups, 1.0, grid)
+    assert O.rel_l2(spec, ref) < SPEC_TOL
+    assert O.rel_l2(spec[:, :, 128:136], ref[:, :, 128:136]) < SPEC_TOL  # the narrow tile
+
+
 def test_tensor_form_long_accumulation_random_points():
     """N = 2^18 decaying-Gaussian particles in 16 h-bins on a 64^3 lattice
     (8192 particles ... per item, long TMEM accumulation with flushes);
