@@ -281,24 +281,28 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16};" ::"r"(taddr),
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
         "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
-        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]),
+        "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]),
+        "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
         : "memory");
 }
 
@@ -322,22 +326,81 @@ __device__ __forceinline__ float2 unit_phase(uint32_t q) {
     return make_float2(c, -s);
 }
 
-// Two complex values (already scaled by 2^12) -> FP16 hi and lo pairs.
-__device__ __forceinline__ uint2 pack_hi_lo(float2 z0, float2 z1, uint2* lo_out) {
-    const __half2 h0 = __floats2half2_rn(z0.x, z0.y);
-    const __half2 h1 = __floats2half2_rn(z1.x, z1.y);
+__device__ __forceinline__ uint32_t h2_bits(__half2 h) { return *reinterpret_cast<const uint32_t*>(&h); }
+
+// A producer's two particles as packed pairs: X = (Re z0, Re z1), Y = (Im z0,
+// Im z1), already scaled by 2^12.  split_pair: FP16 hi and lo of (Re, Im) for
+// each particle (x: particle 0, y: particle 1); the residuals are packed FMAs.
+__device__ __forceinline__ void split_pair(float2 X, float2 Y, uint2& hi, uint2& lo) {
+    const __half2 h0 = __floats2half2_rn(X.x, Y.x), h1 = __floats2half2_rn(X.y, Y.y);
     const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
-    const __half2 l0 = __floats2half2_rn(z0.x - f0.x, z0.y - f0.y);
-    const __half2 l1 = __floats2half2_rn(z1.x - f1.x, z1.y - f1.y);
-    lo_out->x = *reinterpret_cast<const uint32_t*>(&l0);
-    lo_out->y = *reinterpret_cast<const uint32_t*>(&l1);
-    return make_uint2(*reinterpret_cast<const uint32_t*>(&h0), *reinterpret_cast<const uint32_t*>(&h1));
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 dx = __ffma2_rn(make_float2(f0.x, f1.x), m1, X);
+    const float2 dy = __ffma2_rn(make_float2(f0.y, f1.y), m1, Y);
+    hi = make_uint2(h2_bits(h0), h2_bits(h1));
+    lo = make_uint2(h2_bits(__floats2half2_rn(dx.x, dy.x)), h2_bits(__floats2half2_rn(dx.y, dy.y)));
+}
+
+// One step of both particles' chains: z <- z (R q), then q <- q rho (GAUSS;
+// without it q = 1).  Packed: X' = X Rx - Y Ry, Y' = X Ry + Y Rx; NRY = -RY.
+template <bool GAUSS>
+__device__ __forceinline__ void rotate_pair(float2& X, float2& Y, float2 RX, float2 RY, float2 NRY, float2& Q,
+                                            float2 RHO) {
+    float2 rx = RX, ry = RY, nry = NRY;
+    if constexpr (GAUSS) {
+        rx = __fmul2_rn(RX, Q);
+        ry = __fmul2_rn(RY, Q);
+        nry = __fmul2_rn(NRY, Q);
+        Q = __fmul2_rn(Q, RHO);
+    }
+    const float2 nx = __ffma2_rn(X, rx, __fmul2_rn(Y, nry));
+    const float2 ny = __ffma2_rn(X, ry, __fmul2_rn(Y, rx));
+    X = nx;
+    Y = ny;
 }
 
 __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_second) {
     // (re, im) -> (re, -im) when negate_second, else (im, re)
     if (negate_second) return h ^ 0x80000000u;
     return (h >> 16) | (h << 16);
+}
+
+// An A unit's 8 rows (b moving away from 0: row0 + i, or row0 + 7 - i when
+// b < 0) for its two particles, from the chain start (X, Y).  col is the
+// pair's byte offset within a 128-byte operand row.
+template <bool GAUSS>
+__device__ __forceinline__ void a_chain(uint8_t* ahi, uint8_t* alo, int row0, bool up, int col, float2 X, float2 Y,
+                                        float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int off = sw128(row0 + (up ? i : 7 - i), col >> 4) + (col & 15);
+        uint2 hi, lo;
+        split_pair(X, Y, hi, lo);
+        *reinterpret_cast<uint2*>(ahi + off) = hi;
+        *reinterpret_cast<uint2*>(alo + off) = lo;
+        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
+    }
+}
+
+// A B unit's 8 c values for its two particles: row_re + i holds (Re B, -Im B),
+// row_im + i holds (Im B, Re B).
+template <bool GAUSS>
+__device__ __forceinline__ void b_chain(uint8_t* bhi, uint8_t* blo, int row_re, int row_im, int col, float2 X,
+                                        float2 Y, float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int re_off = sw128(row_re + i, col >> 4) + (col & 15);
+        const int im_off = sw128(row_im + i, col >> 4) + (col & 15);
+        uint2 hi, lo;
+        split_pair(X, Y, hi, lo);
+        *reinterpret_cast<uint2*>(bhi + re_off) = make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
+        *reinterpret_cast<uint2*>(blo + re_off) = make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
+        *reinterpret_cast<uint2*>(bhi + im_off) =
+            make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
+        *reinterpret_cast<uint2*>(blo + im_off) =
+            make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
+        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
+    }
 }
 
 // Persistent: CTA b walks items b, b + gridDim.x, ... of the longest-first
@@ -443,7 +506,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             const TcItem I = tc_item<NMAX>(a, it);
             const size_t mk = (size_t)I.job->kx * I.job->ky;
             double* acc = I.job->acc;
-            const double wmax = I.job->wmax;
+            // the accumulator and the total hold 2^24 x the sum (units of the
+            // operand scale); the exact 2^-24 is applied with W at the dump
+            const double dump_scale = I.job->wmax * (double)kInvProductScale;
             const int rho = I.m_tile * kM + row;
             const int c0 = I.n_tile * SH::kNc;
             const int ncols = 2 * I.nc;
@@ -459,27 +524,40 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 // dumped into the FP64 accumulator (and at the item's end)
                 const bool first = (kk % kDumpFlushes) == 0;
                 const bool dump = (kk % kDumpFlushes) == kDumpFlushes - 1 || kk == I.n_chunks - 1;
+                // 32 columns per round trip.  ncols is a multiple of 16, so the
+                // last trip may carry 16 columns past ncols: they stay inside
+                // the accumulator and total regions, are never dumped, and the
+                // total's copy is overwritten by the next item's first flush.
 #pragma unroll 1
-                for (int cc = 0; cc < ncols / 16; ++cc) {
-                    float dv[16], tt[16];
-                    tmem_ld16(acc_col + cc * 16, dv);
-                    if (!first) tmem_ld16(lane_base + kColTotal + cc * 16, tt);
-                    tmem_wait_ld();
+                for (int cc = 0; cc < ncols; cc += 32) {
+                    float tt[32];
+                    if (first) {
+                        tmem_ld32(acc_col + cc, tt);
+                        tmem_wait_ld();
+                    } else {
+                        float dv[32];
+                        tmem_ld32(acc_col + cc, dv);
+                        tmem_ld32(lane_base + kColTotal + cc, tt);
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const float v = dv[i] * kInvProductScale;
-                        tt[i] = first ? v : tt[i] + v;
+                        for (int i = 0; i < 32; i += 2) {
+                            const float2 t2 = __fadd2_rn(make_float2(tt[i], tt[i + 1]), make_float2(dv[i], dv[i + 1]));
+                            tt[i] = t2.x;
+                            tt[i + 1] = t2.y;
+                        }
                     }
                     if (!dump) {
-                        tmem_st16(lane_base + kColTotal + cc * 16, tt);
+                        tmem_st32(lane_base + kColTotal + cc, tt);
                     } else {
                         // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are contiguous
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const int n = cc * 16 + i;
-                            const int im = n >= I.nc ? 1 : 0;
-                            const int c = c0 + n - im * I.nc;
-                            atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * wmax);
+                        for (int i = 0; i < 32; ++i) {
+                            const int n = cc + i;
+                            if (n < ncols) {
+                                const int im = n >= I.nc ? 1 : 0;
+                                const int c = c0 + n - im * I.nc;
+                                atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
+                            }
                         }
                     }
                 }
@@ -574,44 +652,38 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                                 mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)))
                     break;
                 uint8_t* st = smem + buf * kStageBytes;
-                float2 z[2], R[2];
-                float q[2], rq[2];
+                // the thread's two particles as packed pairs (see split_pair)
+                float2 X, Y, RX, RY, Q = make_float2(1.f, 1.f), RHO = make_float2(1.f, 1.f);
+                const int col = 8 * pp;  // byte offset of the pair within a 128-byte operand row
                 if (has_a) {
                     // ---- A: rows rc*8 .. rc*8+7, particles 2pp, 2pp+1 (amp includes 2^12)
+                    float v[2][5];
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         float sn, cs;
                         __sincosf(turns_to_radians((uint32_t)a_x * pqx[e] + (uint32_t)b_s * pqy[e]), &sn, &cs);
-                        float g = pamp[e];
-                        R[e] = a_up ? pry[e] : make_float2(pry[e].x, -pry[e].y);
+                        float g = pamp[e], q = 1.f;
                         if (gauss) {
                             g *= exp2f(pgam[e] * (float)(a_x * a_x + b_s * b_s));
-                            q[e] = exp2f(pgam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
-                            rq[e] = prho2[e];
-                        } else {
-                            q[e] = 1.f;
-                            rq[e] = 1.f;
+                            q = exp2f(pgam[e] * (float)(2 * (a_up ? b_s : -b_s) + 1));
                         }
-                        z[e] = make_float2(g * cs, -g * sn);
+                        v[e][0] = g * cs;
+                        v[e][1] = -g * sn;
+                        v[e][2] = pry[e].x;
+                        v[e][3] = a_up ? pry[e].y : -pry[e].y;
+                        v[e][4] = q;
                     }
-                    uint8_t* ahi = st;
-                    uint8_t* alo = st + kABytes;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int r = a_up ? i : 7 - i;
-                        const int off = sw128(rc * 8 + r, pp >> 1) + (pp & 1) * 8;
-                        uint2 lo;
-                        const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                        *reinterpret_cast<uint2*>(ahi + off) = hi;
-                        *reinterpret_cast<uint2*>(alo + off) = lo;
-#pragma unroll
-                        for (int e = 0; e < 2; ++e) {
-                            const float rx = R[e].x * q[e], ry = R[e].y * q[e];
-                            const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
-                            const float ny = fmaf(z[e].x, ry, z[e].y * rx);
-                            z[e] = make_float2(nx, ny);
-                            q[e] *= rq[e];
-                        }
+                    X = make_float2(v[0][0], v[1][0]);
+                    Y = make_float2(v[0][1], v[1][1]);
+                    RX = make_float2(v[0][2], v[1][2]);
+                    RY = make_float2(v[0][3], v[1][3]);
+                    const float2 NRY = make_float2(-RY.x, -RY.y);
+                    if (gauss) {
+                        Q = make_float2(v[0][4], v[1][4]);
+                        RHO = make_float2(prho2[0], prho2[1]);
+                        a_chain<true>(st, st + kABytes, rc * 8, a_up, col, X, Y, RX, RY, NRY, Q, RHO);
+                    } else {
+                        a_chain<false>(st, st + kABytes, rc * 8, a_up, col, X, Y, RX, RY, NRY, Q, RHO);
                     }
                 } else {
                     // ---- B: c chunks cb and cb + 8 of the n-tile (8 c values each),
@@ -620,49 +692,36 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     // Chunks at or beyond nc are not read by the MMA (N = 2 nc).
                     uint8_t* bhi = st + 2 * kABytes;
                     uint8_t* blo = bhi + SH::kBBytes;
+                    RX = make_float2(prz[0].x, prz[1].x);
+                    RY = make_float2(prz[0].y, prz[1].y);
+                    const float2 NRY = make_float2(-RY.x, -RY.y);
+                    if (gauss) RHO = make_float2(prho2[0], prho2[1]);
 #pragma unroll 1
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.nc) break;
                         const int c_s = I.n_tile * SH::kNc + chunk * 8;
+                        float v[2][3];
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
                             float sn, cs;
                             __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
-                            float g = kOperandScale;
-                            R[e] = prz[e];
+                            float g = kOperandScale, q = 1.f;
                             if (gauss) {
                                 g *= exp2f(pgam[e] * (float)(c_s * c_s));
-                                q[e] = exp2f(pgam[e] * (float)(2 * c_s + 1));
-                                rq[e] = prho2[e];
-                            } else {
-                                q[e] = 1.f;
-                                rq[e] = 1.f;
+                                q = exp2f(pgam[e] * (float)(2 * c_s + 1));
                             }
-                            z[e] = make_float2(g * cs, -g * sn);
+                            v[e][0] = g * cs;
+                            v[e][1] = -g * sn;
+                            v[e][2] = q;
                         }
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            uint2 lo;
-                            const uint2 hi = pack_hi_lo(z[0], z[1], &lo);
-                            const int re_off = sw128(chunk * 8 + i, pp >> 1) + (pp & 1) * 8;
-                            const int im_off = sw128(I.nc + chunk * 8 + i, pp >> 1) + (pp & 1) * 8;
-                            *reinterpret_cast<uint2*>(bhi + re_off) =
-                                make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
-                            *reinterpret_cast<uint2*>(blo + re_off) =
-                                make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
-                            *reinterpret_cast<uint2*>(bhi + im_off) =
-                                make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
-                            *reinterpret_cast<uint2*>(blo + im_off) =
-                                make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
-#pragma unroll
-                            for (int e = 0; e < 2; ++e) {
-                                const float rx = R[e].x * q[e], ry = R[e].y * q[e];
-                                const float nx = fmaf(z[e].x, rx, -z[e].y * ry);
-                                const float ny = fmaf(z[e].x, ry, z[e].y * rx);
-                                z[e] = make_float2(nx, ny);
-                                q[e] *= rq[e];
-                            }
+                        X = make_float2(v[0][0], v[1][0]);
+                        Y = make_float2(v[0][1], v[1][1]);
+                        if (gauss) {
+                            Q = make_float2(v[0][2], v[1][2]);
+                            b_chain<true>(bhi, blo, chunk * 8, I.nc + chunk * 8, col, X, Y, RX, RY, NRY, Q, RHO);
+                        } else {
+                            b_chain<false>(bhi, blo, chunk * 8, I.nc + chunk * 8, col, X, Y, RX, RY, NRY, Q, RHO);
                         }
                     }
                 }
