@@ -132,9 +132,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c4", "c5"], default="c2",
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c3w", "c4", "c5"], default="c2",
                    help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
-                        "N=2^17, 128^3, 4 h-bins (profiling cases)")
+                        "N=2^17, 128^3, 4 h-bins; c3w: the same on 256^3 (the 128x256 tensor tile) (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -153,6 +153,10 @@ def workload(name):
     if name == "c5":
         # the first frame of the 8-frame series (every frame has the same shapes)
         return next(W.c5_frames())
+    if name == "c3w":
+        w = W.c3(n=1 << 17, grid=256, bins=4)
+        w["name"] = "C3-wide-small"
+        return w
     if name == "c3s":
         w = W.c3(n=1 << 17, grid=128, bins=4)
         w["name"] = "C3-small"

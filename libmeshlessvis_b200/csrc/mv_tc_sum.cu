@@ -261,11 +261,6 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;
 }
 
-// Byte offset of 16-byte chunk `chunk` of row `row` in a 128-byte-swizzled operand.
-__device__ __forceinline__ int sw128(int row, int chunk) {
-    return (row >> 3) * kAtomBytes + (row & 7) * kRowBytes + ((chunk ^ (row & 7)) << 4);
-}
-
 __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                         uint32_t accumulate) {
     asm volatile(
@@ -365,39 +360,43 @@ __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_secon
     return (h >> 16) | (h << 16);
 }
 
-// An A unit's 8 rows (b moving away from 0: row0 + i, or row0 + 7 - i when
-// b < 0) for its two particles, from the chain start (X, Y).  col is the
-// pair's byte offset within a 128-byte operand row.
-template <bool GAUSS>
-__device__ __forceinline__ void a_chain(uint8_t* ahi, uint8_t* alo, int row0, bool up, int col, float2 X, float2 Y,
-                                        float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
+// Swizzled offsets: row r (a multiple of 8 plus K, K < 8) of an operand,
+// pair column col = 8 pp: r * 128 + ((col >> 4) ^ K) * 16 + (col & 15).  With
+// base = 128 * (r - K) + (col & 15) and c16 = col & ~15 fixed per thread, a
+// chain's step K adds K * 128 + (c16 ^ 16 K): one XOR and one add per step.
+__device__ __forceinline__ int sw_step(int c16, int K) { return K * kRowBytes + (c16 ^ (K << 4)); }
+
+// An A unit's 8 rows for its two particles (b moving away from 0: K = i when
+// UP, 7 - i otherwise), from the chain start (X, Y); lo goes kABytes after hi.
+template <bool GAUSS, bool UP>
+__device__ __forceinline__ void a_chain(uint8_t* base, int c16, float2 X, float2 Y, float2 RX, float2 RY, float2 NRY,
+                                        float2 Q, float2 RHO) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int off = sw128(row0 + (up ? i : 7 - i), col >> 4) + (col & 15);
+        uint8_t* p = base + sw_step(c16, UP ? i : 7 - i);
         uint2 hi, lo;
         split_pair(X, Y, hi, lo);
-        *reinterpret_cast<uint2*>(ahi + off) = hi;
-        *reinterpret_cast<uint2*>(alo + off) = lo;
+        *reinterpret_cast<uint2*>(p) = hi;
+        *reinterpret_cast<uint2*>(p + kABytes) = lo;
         if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
     }
 }
 
-// A B unit's 8 c values for its two particles: row_re + i holds (Re B, -Im B),
-// row_im + i holds (Im B, Re B).
+// A B unit's 8 c values for its two particles: (Re B, -Im B) at re_base (a
+// Re F row), (Im B, Re B) at im_base (the Im F row); lo goes lo_gap after hi.
 template <bool GAUSS>
-__device__ __forceinline__ void b_chain(uint8_t* bhi, uint8_t* blo, int row_re, int row_im, int col, float2 X,
-                                        float2 Y, float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
+__device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int lo_gap, int c16, float2 X, float2 Y,
+                                        float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int re_off = sw128(row_re + i, col >> 4) + (col & 15);
-        const int im_off = sw128(row_im + i, col >> 4) + (col & 15);
+        const int off = sw_step(c16, i);
         uint2 hi, lo;
         split_pair(X, Y, hi, lo);
-        *reinterpret_cast<uint2*>(bhi + re_off) = make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
-        *reinterpret_cast<uint2*>(blo + re_off) = make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
-        *reinterpret_cast<uint2*>(bhi + im_off) =
-            make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
-        *reinterpret_cast<uint2*>(blo + im_off) =
+        *reinterpret_cast<uint2*>(re_base + off) = make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
+        *reinterpret_cast<uint2*>(re_base + off + lo_gap) =
+            make_uint2(h2_swap_negate(lo.x, true), h2_swap_negate(lo.y, true));
+        *reinterpret_cast<uint2*>(im_base + off) = make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
+        *reinterpret_cast<uint2*>(im_base + off + lo_gap) =
             make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
         if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
     }
@@ -678,12 +677,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     RX = make_float2(v[0][2], v[1][2]);
                     RY = make_float2(v[0][3], v[1][3]);
                     const float2 NRY = make_float2(-RY.x, -RY.y);
+                    uint8_t* base = st + rc * 8 * kRowBytes + (col & 15);
+                    const int c16 = col & ~15;
                     if (gauss) {
                         Q = make_float2(v[0][4], v[1][4]);
                         RHO = make_float2(prho2[0], prho2[1]);
-                        a_chain<true>(st, st + kABytes, rc * 8, a_up, col, X, Y, RX, RY, NRY, Q, RHO);
+                        if (a_up) a_chain<true, true>(base, c16, X, Y, RX, RY, NRY, Q, RHO);
+                        else a_chain<true, false>(base, c16, X, Y, RX, RY, NRY, Q, RHO);
                     } else {
-                        a_chain<false>(st, st + kABytes, rc * 8, a_up, col, X, Y, RX, RY, NRY, Q, RHO);
+                        if (a_up) a_chain<false, true>(base, c16, X, Y, RX, RY, NRY, Q, RHO);
+                        else a_chain<false, false>(base, c16, X, Y, RX, RY, NRY, Q, RHO);
                     }
                 } else {
                     // ---- B: c chunks cb and cb + 8 of the n-tile (8 c values each),
@@ -691,7 +694,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     // Re F columns), rows [nc, 2 nc) (Im B, Re B) (the Im F columns).
                     // Chunks at or beyond nc are not read by the MMA (N = 2 nc).
                     uint8_t* bhi = st + 2 * kABytes;
-                    uint8_t* blo = bhi + SH::kBBytes;
                     RX = make_float2(prz[0].x, prz[1].x);
                     RY = make_float2(prz[0].y, prz[1].y);
                     const float2 NRY = make_float2(-RY.x, -RY.y);
@@ -717,11 +719,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         }
                         X = make_float2(v[0][0], v[1][0]);
                         Y = make_float2(v[0][1], v[1][1]);
+                        // nc and chunk * 8 are multiples of 8: row K of the chain is K within its atom
+                        uint8_t* re_base = bhi + chunk * 8 * kRowBytes + (col & 15);
+                        uint8_t* im_base = bhi + (I.nc + chunk * 8) * kRowBytes + (col & 15);
+                        const int c16 = col & ~15;
                         if (gauss) {
                             Q = make_float2(v[0][2], v[1][2]);
-                            b_chain<true>(bhi, blo, chunk * 8, I.nc + chunk * 8, col, X, Y, RX, RY, NRY, Q, RHO);
+                            b_chain<true>(re_base, im_base, SH::kBBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
                         } else {
-                            b_chain<false>(bhi, blo, chunk * 8, I.nc + chunk * 8, col, X, Y, RX, RY, NRY, Q, RHO);
+                            b_chain<false>(re_base, im_base, SH::kBBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
                         }
                     }
                 }
