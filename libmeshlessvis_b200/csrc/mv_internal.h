@@ -138,7 +138,8 @@ struct TcJob {
     int n;        // particles
     int k_chunk;  // particles per item (multiple of 32)
     int gauss;    // per-particle Gaussian factors (GAUSSIAN_DECAYING with radii)
-    int pad[2];
+    int nc_tile;  // c values per n-tile (a multiple of 8; the last tile may be narrower)
+    int pad;
 };
 
 struct TensorPlan {

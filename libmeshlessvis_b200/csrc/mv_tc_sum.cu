@@ -148,7 +148,7 @@ struct TcItem {
     int m_tile, n_tile;
     int kb, ke;
     int n_stages, n_chunks;
-    int nc;  // c values of this n-tile (a multiple of 8); the MMA's N is 2 nc
+    int c0, nc;  // the n-tile's first c and c values (a multiple of 8); the MMA's N is 2 nc
 };
 
 template <int NMAX>
@@ -165,7 +165,8 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
     r.ke = min(r.job->n, r.kb + r.job->k_chunk);
     r.n_stages = max(0, (r.ke - r.kb + kKp - 1) / kKp);
     r.n_chunks = (r.n_stages + a.flush_stages - 1) / a.flush_stages;
-    r.nc = min(Shape<NMAX>::kNc, r.job->lz_tc - r.n_tile * Shape<NMAX>::kNc);
+    r.c0 = r.n_tile * r.job->nc_tile;
+    r.nc = min(r.job->nc_tile, r.job->lz_tc - r.c0);
     return r;
 }
 
@@ -509,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             // operand scale); the exact 2^-24 is applied with W at the dump
             const double dump_scale = I.job->wmax * (double)kInvProductScale;
             const int rho = I.m_tile * kM + row;
-            const int c0 = I.n_tile * SH::kNc;
+            const int c0 = I.c0;
             const int ncols = 2 * I.nc;
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
@@ -702,7 +703,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.nc) break;
-                        const int c_s = I.n_tile * SH::kNc + chunk * 8;
+                        const int c_s = I.c0 + chunk * 8;
                         float v[2][3];
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
@@ -943,9 +944,14 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.ky = ky;
         j.lz_tc = lz_tc;
         const int wide = lz_tc > Shape<128>::kNc ? 1 : 0;  // NMAX = 256 beyond 64 tensor planes
-        const int nc_tile = wide ? Shape<256>::kNc : Shape<128>::kNc;
+        // equal n-tiles of at most NMAX / 2 c values: 192 planes -> 96 + 96
+        // (two N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by
+        // its shared-memory operand reads)
+        const int nc_max = wide ? Shape<256>::kNc : Shape<128>::kNc;
+        j.n_ntiles = (lz_tc + nc_max - 1) / nc_max;
+        j.nc_tile = ((lz_tc + j.n_ntiles - 1) / j.n_ntiles + 7) / 8 * 8;
+        j.n_ntiles = (lz_tc + j.nc_tile - 1) / j.nc_tile;
         j.n_mtiles = (int)((long long)kx * ky / kM);
-        j.n_ntiles = (lz_tc + nc_tile - 1) / nc_tile;
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;

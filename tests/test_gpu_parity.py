@@ -262,16 +262,18 @@ def test_tensor_form_matches_fp64(case):
 
 
 @pytest.mark.parametrize("case", ["gauss_decaying_radii", "wendland_uniform_radius"])
-def test_tensor_form_two_n_tiles_of_unequal_width(case):
-    """A 32x32x272 lattice: the tensor planes c < 136 split into an n-tile of
-    128 c values (MMA N = 256) and one of 8 (N = 16, the smallest MMA width)."""
+@pytest.mark.parametrize("grid", [(32, 32, 272), (32, 32, 16)])
+def test_tensor_form_uneven_and_narrowest_n_tiles(case, grid):
+    """32x32x272: the tensor planes c < 136 split into n-tiles of 72 and 64 c
+    values (MMA N = 144 and 128); 32x32x16: one tile of 8 (N = 16, the
+    smallest MMA width)."""
     rng = np.random.default_rng(23)
     groups = _tc_groups(rng, 2001)[case]
-    grid = (32, 32, 272)
     spec, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
     ref = O.spectrum_grid(groups, 1.0, grid)
     assert O.rel_l2(spec, ref) < SPEC_TOL
-    assert O.rel_l2(spec[:, :, 128:136], ref[:, :, 128:136]) < SPEC_TOL  # the narrow tile
+    lz = grid[2] // 2
+    assert O.rel_l2(spec[:, :, lz - 8:lz], ref[:, :, lz - 8:lz]) < SPEC_TOL  # the last tile's planes
 
 
 def test_tensor_form_long_accumulation_random_points():
