@@ -136,6 +136,8 @@ def parse():
                    help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
                         "N=2^17, 128^3, 4 h-bins; c3w: the same on 256^3 (the 128x256 tensor tile) (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
+    p.add_argument("--autotune", action="store_true",
+                   help="run the library's autotuner (vis_autotune_spectrum) on the workload before the warm-up")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--compare-forms", action="store_true",
@@ -397,6 +399,16 @@ def run_ours(args):
         sp.compute(cfg, ds, form)
         sp.render_views(cfg, u, v, d_images=d_images.data_ptr(), to_host=False)
 
+    tuned = None
+    if args.autotune:
+        # outside the timed region: times the candidates, keeps the best for this shape
+        import ctypes
+
+        best_ms = sp.autotune(cfg, ds, form)
+        vals = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
+        lib.vis_autotune_lookup(M.int3(*w["grid"]), n, len(w["groups"]), form, *[ctypes.byref(x) for x in vals])
+        tuned = {"plain_waves": vals[0].value, "tensor_waves": vals[1].value, "tensor_flush_stages": vals[2].value,
+                 "best_sum_ms": best_ms}
     for _ in range(max(3, args.warmup)):
         step()
     cfg.synchronize()
@@ -503,7 +515,7 @@ def run_ours(args):
                 "config": {"workload": w["name"], "particles": n, "grid": list(w["grid"]),
                            "half_spectrum": g, "views": nv, "image": [nx, ny], "form": args.form,
                            "l2": "flushed between timed steps (256 MB write outside the event pair)",
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"replicas x{world}", "autotune": tuned},
                 "views_per_s": views_per_s,
                 "stages_ms_per_step": {name: stage_t[st][0] / args.steps for st, name in STAGE_NAMES.items()},
                 "roofline": roofline, "clocks": clk, "gpu_launches": int(launches),

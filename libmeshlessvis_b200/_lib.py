@@ -6,7 +6,7 @@ at import time when the shared library has not been built, so no caller can
 silently run without the CUDA code.
 """
 import ctypes
-from ctypes import POINTER, c_bool, c_char_p, c_float, c_int, c_void_p
+from ctypes import POINTER, c_bool, c_char_p, c_float, c_int, c_longlong, c_void_p
 from pathlib import Path
 
 import numpy as np
@@ -107,6 +107,9 @@ SIGNATURES = {
     "vis_spectrum_grid_size": (int3, [c_void_p]),
     "vis_spectrum_device_data": (c_void_p, [c_void_p]),
     "vis_spectrum_compute": (c_int, [c_void_p, PConfig, PDataset, c_int]),
+    "vis_autotune_spectrum": (c_int, [c_void_p, PConfig, PDataset, c_int, POINTER(c_float)]),
+    "vis_autotune_lookup": (c_int, [int3, c_longlong, c_int, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "vis_autotune_clear": (None, []),
     "vis_spectrum_copy_to_host": (c_int, [c_void_p, PConfig, c_void_p]),
     "vis_spectrum_render_views": (c_int, [c_void_p, PConfig, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "vis_config_enable_kernel_timing": (c_int, [PConfig, c_int]),

@@ -822,6 +822,10 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
     if (!sp || !s || !ds || (ds->number_of_groups > 0 && !ds->groups))
         return set_error(kInvalidValue, "vis_spectrum_compute: NULL or unknown argument");
     if (form < VIS_FORM_AUTO || form > VIS_FORM_TENSOR) return set_error(kInvalidValue, "vis_spectrum_compute: bad form");
+    // the autotuned launch parameters of this shape, if any (else the defaults)
+    long long n_total = 0;
+    for (int g = 0; g < ds->number_of_groups; ++g) n_total += std::max(0, ds->groups[g].number_of_terms);
+    TuneScope tune(tuned_params(sp->grid.x, sp->grid.y, sp->grid.z, n_total, ds->number_of_groups, form));
     std::vector<SumRequest> tc_groups, plain_groups;
     for (int g = 0; g < ds->number_of_groups; ++g) {
         const Group& grp = ds->groups[g];

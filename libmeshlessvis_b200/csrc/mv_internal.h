@@ -162,6 +162,7 @@ struct TensorPlan {
     size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
     const void* d_jobs = nullptr;
     const void* d_items = nullptr;
+    int flush = 8;  // stages per TMEM accumulation chain, as planned
 };
 
 struct TensorWorkspace {
@@ -189,6 +190,24 @@ void timer_begin(KernelTimer* timer, int stage, cudaStream_t stream);
 void timer_end(KernelTimer* timer, int stage, cudaStream_t stream);
 
 int device_sm_count();
+
+// Launch parameters chosen per workload shape by the autotuner
+// (vis_autotune_spectrum, mv_tune.cu); defaults otherwise.  Only parameters
+// that leave results within tolerance are tuned.
+struct TuneParams {
+    int plain_waves = 6;  // plain form: split-K until the grid holds ~plain_waves blocks per SM
+    int tc_waves = 4;     // tensor form: particle splits until the items make ~tc_waves waves
+    int tc_flush = 8;     // tensor form: stages per TMEM accumulation chain (4 or 8)
+};
+// The parameters in force on this thread: set by TuneScope around a compute.
+const TuneParams& active_tune();
+struct TuneScope {
+    explicit TuneScope(const TuneParams& p);
+    ~TuneScope();
+    TuneParams saved;
+};
+// The table entry for a spectrum shape, or the defaults.
+TuneParams tuned_params(int kx, int ky, int kz, long long n_total, int n_groups, int form);
 
 // Statistics of a registered group, recorded by vis_register_meshless_dataset
 // and keyed by the group's device particle pointer; all -1 if unknown.

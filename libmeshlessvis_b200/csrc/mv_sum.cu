@@ -560,9 +560,10 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     if (threads > (1LL << 31) - 1) return set_error(kInvalidValue, "lattice too large");
     const long long blocks_f = (threads + kThreads - 1) / kThreads;
 
-    // Split the particle range until the grid holds ~6 blocks per SM (two
-    // waves of the 3 resident blocks), keeping at least 4 tiles per split.
-    const long long target = (long long)device_sm_count() * 6;
+    // Split the particle range until the grid holds ~plain_waves blocks per SM
+    // (default 6: three waves of the 2 resident blocks; the autotuner may pick
+    // another), keeping at least 4 tiles per split.
+    const long long target = (long long)device_sm_count() * active_tune().plain_waves;
     long long max_splits = std::max<long long>(1, (req.n + 4 * kThreads - 1) / (4 * kThreads));
     long long splits = std::min<long long>(std::max<long long>(1, (target + blocks_f - 1) / blocks_f), max_splits);
     splits = std::min<long long>(splits, 65535);

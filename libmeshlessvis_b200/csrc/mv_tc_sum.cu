@@ -851,15 +851,15 @@ bool is_spectrum_lattice(const Lattice& L) {
            L.m[6] == 0 && L.m[7] == 0;
 }
 
-// Stages per TMEM accumulation chain before the flush into the compensated
-// total: MV_TC_FLUSH_STAGES (1..1024) overrides the default.
+// Stages per TMEM accumulation chain before a flush into the FP32 total:
+// MV_TC_FLUSH_STAGES (1..1024) overrides the tuned (or default) value.
 int tc_flush_stages() {
-    static const int v = [] {
+    static const int env = [] {
         const char* e = std::getenv("MV_TC_FLUSH_STAGES");
         const int x = e ? std::atoi(e) : 0;
-        return (x >= 1 && x <= 1024) ? x : 8;
+        return (x >= 1 && x <= 1024) ? x : 0;
     }();
-    return v;
+    return env ? env : active_tune().tc_flush;
 }
 
 }  // namespace
@@ -904,6 +904,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     };
     std::vector<Item> items;
     const int flush = tc_flush_stages();
+    plan.flush = flush;
     for (size_t g = 0; g < groups.size(); ++g) {
         const SumRequest& r = groups[g];
         const Lattice& L = r.lat;
@@ -955,10 +956,10 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
-        // particle splits: enough items per group for ~4 waves on its own, at
-        // least 64 stages each
+        // particle splits: enough items per group for ~tc_waves waves on its
+        // own (default 4), at least 64 stages each
         const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
-        const long long target = (long long)device_sm_count() * 4;
+        const long long target = (long long)device_sm_count() * active_tune().tc_waves;
         long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
         splits = std::min<long long>(splits, std::max<long long>(1, (r.n + 64 * kKp - 1) / (64 * kKp)));
         const long long chunk = ((r.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
@@ -1057,7 +1058,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             a.jobs = static_cast<const TcJob*>(plan.d_jobs);
             a.items = static_cast<const int2*>(plan.d_items) + (wide ? plan.n_narrow : 0);
             a.n_items = wide ? (int)plan.items.size() - plan.n_narrow : plan.n_narrow;
-            a.flush_stages = tc_flush_stages();
+            a.flush_stages = plan.flush;
             a.error_flag = error_flag;
             if (a.n_items == 0) continue;
             const int grid = std::min<int>(a.n_items, device_sm_count());

@@ -1,0 +1,133 @@
+// Autotuner: picks, per spectrum shape, the launch parameters that the
+// kernels otherwise derive from fixed rules (TuneParams in mv_internal.h):
+//   plain_waves  split-K of the plain form, in blocks per SM: 2, 4, 6, 8
+//   tc_waves     particle splits of the tensor form, in waves: 2, 4, 8
+//   tc_flush     tensor-core accumulation chain, in stages: 4, 8 (longer
+//                chains lose accuracy, so they are not candidates)
+// vis_autotune_spectrum times each candidate on the caller's own data through
+// the public compute path (one warm-up and one timed run, CUDA events on the
+// config's stream), one parameter at a time starting from the defaults, and
+// records the fastest set for the shape: lattice, total particles, number of
+// groups and form.  Later vis_spectrum_compute calls of that shape use it.
+// The table is process-wide; vis_autotune_clear empties it.
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "meshless_vis_b200.h"
+#include "mv_internal.h"
+
+namespace mv {
+namespace {
+
+using TuneKey = std::tuple<int, int, int, long long, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneParams> g_tune_table;
+thread_local TuneParams g_active;
+
+long long dataset_terms(const MeshlessDataset* ds, int* groups) {
+    long long n = 0;
+    *groups = ds->number_of_groups;
+    for (int g = 0; g < ds->number_of_groups; ++g) n += std::max(0, ds->groups[g].number_of_terms);
+    return n;
+}
+
+}  // namespace
+
+const TuneParams& active_tune() { return g_active; }
+TuneScope::TuneScope(const TuneParams& p) : saved(g_active) { g_active = p; }
+TuneScope::~TuneScope() { g_active = saved; }
+
+TuneParams tuned_params(int kx, int ky, int kz, long long n_total, int n_groups, int form) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_table.find(TuneKey(kx, ky, kz, n_total, n_groups, form));
+    return it == g_tune_table.end() ? TuneParams{} : it->second;
+}
+
+}  // namespace mv
+
+using namespace mv;
+
+extern "C" {
+
+int vis_autotune_spectrum(VisSpectrum* sp, VisConfig* vis_config, MeshlessDataset* meshless_dataset, int form,
+                          float* best_ms) {
+    if (!sp || !vis_config || !meshless_dataset)
+        return set_error(kInvalidValue, "vis_autotune_spectrum: NULL argument");
+    const int3 grid = vis_spectrum_grid_size(sp);
+    int rc = kOk;
+    cudaStream_t stream = vis_config_get_stream(vis_config);
+    int groups = 0;
+    const long long n = dataset_terms(meshless_dataset, &groups);
+    const TuneKey key(grid.x, grid.y, grid.z, n, groups, form);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_table.erase(key);  // time every candidate from the defaults
+    }
+    cudaEvent_t e0, e1;
+    rc = check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    if (rc != kOk) return rc;
+    rc = check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    if (rc != kOk) {
+        cudaEventDestroy(e0);
+        return rc;
+    }
+    // one warm-up and one timed run of a candidate; < 0 on error
+    auto time_of = [&](const TuneParams& p) -> float {
+        TuneScope scope(p);
+        if (vis_spectrum_compute(sp, vis_config, meshless_dataset, form) != kOk) return -1.f;
+        cudaEventRecord(e0, stream);
+        if (vis_spectrum_compute(sp, vis_config, meshless_dataset, form) != kOk) return -1.f;
+        cudaEventRecord(e1, stream);
+        if (check_cuda(cudaEventSynchronize(e1), "vis_autotune_spectrum") != kOk) return -1.f;
+        float ms = -1.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    TuneParams best;
+    float best_t = time_of(best);
+    const int plain_c[] = {2, 4, 6, 8}, waves_c[] = {2, 4, 8}, flush_c[] = {8, 4};
+    for (int field = 0; field < 3 && best_t >= 0.f; ++field) {
+        const int* cand = field == 0 ? plain_c : field == 1 ? waves_c : flush_c;
+        const int count = field == 0 ? 4 : field == 1 ? 3 : 2;
+        for (int i = 0; i < count && best_t >= 0.f; ++i) {
+            TuneParams p = best;
+            int& v = field == 0 ? p.plain_waves : field == 1 ? p.tc_waves : p.tc_flush;
+            if (v == cand[i]) continue;
+            v = cand[i];
+            const float t = time_of(p);
+            if (t < 0.f) best_t = -1.f;
+            else if (t < best_t) {
+                best_t = t;
+                best = p;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_t < 0.f) return vis_get_last_error() != kOk ? vis_get_last_error() : set_error(kCudaError, "vis_autotune_spectrum");
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_table[key] = best;
+    }
+    if (best_ms) *best_ms = best_t;
+    return kOk;
+}
+
+int vis_autotune_lookup(int3 grid_size, long long number_of_terms, int number_of_groups, int form, int* plain_waves,
+                        int* tensor_waves, int* tensor_flush_stages) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_table.find(TuneKey(grid_size.x, grid_size.y, grid_size.z, number_of_terms, number_of_groups, form));
+    const TuneParams p = it == g_tune_table.end() ? TuneParams{} : it->second;
+    if (plain_waves) *plain_waves = p.plain_waves;
+    if (tensor_waves) *tensor_waves = p.tc_waves;
+    if (tensor_flush_stages) *tensor_flush_stages = p.tc_flush;
+    return it == g_tune_table.end() ? 0 : 1;
+}
+
+void vis_autotune_clear(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_table.clear();
+}
+
+}  // extern "C"

@@ -204,6 +204,15 @@ class Spectrum:
     def compute(self, config, dataset, form=FORM_AUTO):
         L.check(self.lib, self.lib.vis_spectrum_compute(self.ptr, config.ptr, dataset.ref, int(form)))
 
+    def autotune(self, config, dataset, form=FORM_AUTO):
+        """Times the launch-parameter candidates for this shape on `dataset`
+        (vis_autotune_spectrum) and returns the best time in ms; later
+        computes of the same shape use the chosen parameters."""
+        ms = ctypes.c_float(0.0)
+        L.check(self.lib, self.lib.vis_autotune_spectrum(self.ptr, config.ptr, dataset.ref, int(form),
+                                                         ctypes.byref(ms)))
+        return ms.value
+
     def to_host(self, config):
         out = np.empty(self.shape, dtype=np.complex64)
         L.check(self.lib, self.lib.vis_spectrum_copy_to_host(self.ptr, config.ptr, out.ctypes.data))

@@ -171,3 +171,14 @@ def test_write_ppm_layout_and_flip(tmp_path):
     px = np.frombuffer(data[len(header):], np.uint8).reshape(h, w, 3)
     # vertical flip, as the reference's JPEG writer (vis_noninteractive/main.cpp:31)
     assert (px[2, :, 0] == 255).all() and px[0, 1, 2] == 128
+
+
+def test_autotune_table_starts_with_the_defaults():
+    """Without a tuning run, every shape reports the default launch parameters
+    (plain split-K 6 blocks per SM, tensor splits 4 waves, 8-stage chains)."""
+    lib = L.load()
+    lib.vis_autotune_clear()
+    vals = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
+    tuned = lib.vis_autotune_lookup(L.int3(64, 64, 64), 4096, 2, 0, *[ctypes.byref(v) for v in vals])
+    assert tuned == 0
+    assert [v.value for v in vals] == [6, 4, 8]
