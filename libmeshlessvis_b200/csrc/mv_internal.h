@@ -154,8 +154,8 @@ struct TensorPlan {
         size_t acc_offset;
     };
     std::vector<TcJob> jobs;
-    std::vector<int2> items;  // NMAX = 128 items first (n_narrow of them), then NMAX = 256
-    int n_narrow = 0;
+    std::vector<int2> items;  // 128x128-tile items (n_narrow), CTA-pair items (n_pair), then 128x256
+    int n_narrow = 0, n_pair = 0;
     std::vector<Class> classes;
     std::vector<int> group_class, job_of_group;
     std::vector<size_t> tp_offset;

@@ -100,37 +100,49 @@ constexpr int kFlushWarps = 4;
 constexpr int kLoaderWarp = 1 + kFlushWarps + kProducerWarps;
 constexpr int kThreads = 32 * (kLoaderWarp + 1);
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kColTotal = 256;  // FP32 total: columns [256, 256 + NMAX)
+constexpr uint32_t kColTotal = 256;  // FP32 total: columns [256, 256 + accumulator columns)
 constexpr int kDumpFlushes = 16;  // chain partials summed in FP32 before an FP64 dump
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
 constexpr float kInvProductScale = 1.f / (4096.f * 4096.f);  // 2^-24
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
-// The two tile widths.  NMAX = real accumulator columns of an n-tile (Re | Im
-// of NMAX / 2 c values):
-//   NMAX = 128: two 128-column TMEM accumulators alternate, so the MMAs never
-//               wait for a flush; 3 stages of 64 KB operands;
-//   NMAX = 256: one 256-column accumulator (the MMA waits while a flush reads
-//               it); 2 stages of 96 KB.  The 128x256 MMA reads A once for
-//               twice the work of a 128x128 one, which keeps its operand reads
-//               within the shared-memory port.
-// A job takes NMAX = 128 when its lattice has at most 64 tensor planes.
-template <int NMAX>
+// Tile kinds (template parameter MODE):
+//   kNarrow (lattices with at most 64 tensor planes): 128x128 MMA, two
+//       alternating 128-column TMEM accumulators (the MMAs never wait for a
+//       flush), 3 stages of 64 KB;
+//   kWide: 128x256 MMA, one 256-column accumulator (the MMA waits while a
+//       flush reads it), 2 stages of 96 KB;
+//   kPair: a CTA pair (cluster of 2) runs one 256x256 MMA (tcgen05
+//       cta_group::2): each CTA holds 128 rows of A and the B rows of half the
+//       n-tile's c values, and its 128 accumulator rows of all 256 columns in
+//       its own TMEM.  Each CTA produces the operands of a narrow tile per
+//       stage for twice its work, and the MMA reads 64 B/clk of shared memory
+//       per CTA.  Used where the tensor planes are a multiple of 16 and the
+//       rows a multiple of 256.
+enum TileMode : int { kNarrow = 0, kWide = 1, kPair = 2 };
+
+template <int MODE>
 struct Shape {
-    static constexpr int kNc = NMAX / 2;                      // c values per n-tile
-    static constexpr int kStages = NMAX == 128 ? 3 : 2;
-    static constexpr int kBufs = NMAX == 128 ? 2 : 1;         // TMEM accumulators, NMAX columns each
-    static constexpr int kBBytes = NMAX * kRowBytes;          // B operand: NMAX rows
+    static constexpr int kCtas = MODE == kPair ? 2 : 1;
+    static constexpr int kN = MODE == kNarrow ? 128 : 256;  // accumulator columns: the MMA's N at most
+    static constexpr int kNc = kN / 2;                       // c values per n-tile (at most)
+    static constexpr int kBRows = kN / kCtas;                // B operand rows held by one CTA
+    static constexpr int kMTile = kM * kCtas;                // lattice rows per m-tile
+    static constexpr int kStages = MODE == kWide ? 2 : 3;
+    static constexpr int kBufs = MODE == kNarrow ? 2 : 1;    // TMEM accumulators, kN columns each
+    static constexpr int kBBytes = kBRows * kRowBytes;
     static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
-    static constexpr int kChunksPerThread = NMAX / 128;       // 8-c chunks per B producer thread
+    static constexpr int kChunksPerThread = kBRows / 128;    // 8-c chunks per B producer thread
     static constexpr size_t kBarrierOffset = (size_t)kStages * (kStageBytes + kSlotBytes);
     static constexpr size_t kSmemBytes = kBarrierOffset + 256;
 };
-static_assert(Shape<256>::kSmemBytes <= 227 * 1024 && Shape<128>::kSmemBytes <= 227 * 1024, "shared memory");
+static_assert(Shape<kNarrow>::kSmemBytes <= 227 * 1024 && Shape<kWide>::kSmemBytes <= 227 * 1024 &&
+                  Shape<kPair>::kSmemBytes <= 227 * 1024,
+              "shared memory");
 
-// idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t mma_idesc(int n) {
-    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+// idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, M = m, N = n.
+__host__ __device__ constexpr uint32_t mma_idesc(int m, int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 
@@ -148,11 +160,13 @@ struct TcItem {
     int m_tile, n_tile;
     int kb, ke;
     int n_stages, n_chunks;
-    int c0, nc;  // the n-tile's first c and c values (a multiple of 8); the MMA's N is 2 nc
+    int c0, nc;    // the n-tile's first c and c values (a multiple of 8); the MMA's N is 2 nc
+    int bc0, bnc;  // the c values whose B rows this CTA produces: all of them, or one half (kPair)
+    int row0;      // this CTA's first lattice row
 };
 
-template <int NMAX>
-__device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
+template <int MODE>
+__device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     const int2 v = a.items[it];
     TcItem r;
     r.job = a.jobs + v.x;
@@ -167,6 +181,9 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it) {
     r.n_chunks = (r.n_stages + a.flush_stages - 1) / a.flush_stages;
     r.c0 = r.n_tile * r.job->nc_tile;
     r.nc = min(r.job->nc_tile, r.job->lz_tc - r.c0);
+    r.bnc = r.nc / Shape<MODE>::kCtas;
+    r.bc0 = r.c0 + rank * r.bnc;
+    r.row0 = r.m_tile * Shape<MODE>::kMTile + rank * kM;
     return r;
 }
 
@@ -186,11 +203,32 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Arrive on the barrier at the same shared-memory offset in the pair's CTA 0
+// (the leader, which issues the pair's MMAs); release at cluster scope.
+__device__ __forceinline__ void mbar_arrive_leader(uint64_t* bar) {
+    asm volatile(
+        "{\n\t.reg .b32 ra;\n\t"
+        "mapa.shared::cluster.u32 ra, %0, 0;\n\t"
+        "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}" ::"r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Every thread of both CTAs of the cluster (aligned: the whole warp).
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity)
@@ -207,7 +245,7 @@ __device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t pa
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
@@ -262,19 +300,46 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;
 }
 
+// CTAS = 2: the pair's MMA (cta_group::2), issued by one thread of CTA 0; the
+// descriptors name this CTA's shared-memory offsets, which hold the operands
+// in both CTAs (no output lanes disabled).
+template <int CTAS>
 __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                         uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
+    if constexpr (CTAS == 1) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+                d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+            "r"(0u), "r"(0u)
+            : "memory");
+    }
 }
 
+// Arrives on bar once the MMAs issued so far are complete; CTAS = 2: on the
+// barrier at the same offset in both CTAs of the pair.
+template <int CTAS>
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
+    if constexpr (CTAS == 1) {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(bar))
+                     : "memory");
+    } else {
+        asm volatile(
+            "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                smem_u32(bar)),
+            "h"((unsigned short)3)
+            : "memory");
+    }
 }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
@@ -403,23 +468,32 @@ __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int 
     }
 }
 
-// Persistent: CTA b walks items b, b + gridDim.x, ... of the longest-first
-// item list.  Every role walks the same items in the same order, and the
-// pipeline's stage and chunk counters (hence mbarrier phases and the TMEM
-// accumulator parity) run on across items; TMEM and the barriers are set up
-// once per CTA.
-template <int NMAX>
+// Persistent: CTA (or CTA pair) b walks items b, b + grid, ... of the
+// longest-first item list.  Every role walks the same items in the same
+// order, and the pipeline's stage and chain counters (hence mbarrier phases
+// and the TMEM accumulator parity) run on across items; TMEM and the barriers
+// are set up once per CTA.
+//
+// kPair: the barriers that gate the pair's MMAs (full, acc_empty) live in CTA
+// 0 and count the arrivals of both CTAs; the MMA's completion (empty,
+// acc_full, drain) is signalled to both CTAs by multicast commits; each CTA's
+// loader, producers and flush warps otherwise work on their own shared memory
+// and TMEM.  Cluster barriers after set-up and before exit keep each CTA's
+// shared memory alive while the other may still signal it.
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
-    using SH = Shape<NMAX>;
-    constexpr int kStages = SH::kStages, kStageBytes = SH::kStageBytes, kBufs = SH::kBufs;
+    using SH = Shape<MODE>;
+    constexpr int kStages = SH::kStages, kStageBytes = SH::kStageBytes, kBufs = SH::kBufs, kCtas = SH::kCtas;
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* slots = smem + kStages * kStageBytes;  // [kStages][kSlotBytes]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SH::kBarrierOffset);
-    uint64_t* full = bars;                   // [kStages] producers -> MMA
+    uint64_t* full = bars;                   // [kStages] producers -> MMA (CTA 0's)
     uint64_t* empty = bars + kStages;        // [kStages] MMA -> producers
     uint64_t* pdata = bars + 2 * kStages;    // [kStages] loader -> producers
-    uint64_t* acc_full = bars + 3 * kStages;   // [kBufs] MMA -> flush: a chain is complete
-    uint64_t* acc_empty = acc_full + 2;         // [kBufs] flush -> MMA: the accumulator has been read
+    uint64_t* sfree = bars + 3 * kStages;    // [kStages] producers -> loader: the slot has been read
+    uint64_t* pfull = bars + 4 * kStages;    // [kStages] kPair, CTA 1: its producers -> its forwarder
+    uint64_t* acc_full = bars + 5 * kStages;   // [kBufs] MMA -> flush: a chain is complete
+    uint64_t* acc_empty = acc_full + 2;         // [kBufs] flush -> MMA (CTA 0's): the accumulator has been read
     uint64_t* drain = acc_full + 4;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(acc_full + 5);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(acc_full + 5) + 1;
@@ -428,6 +502,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     const int warp = tid >> 5;
     const int lane = tid & 31;
     const int flush_stages = a.flush_stages;
+    const int rank = kCtas == 2 ? (int)cluster_rank() : 0;
+    const int unit = blockIdx.x / kCtas, n_units = gridDim.x / kCtas;  // CTA or CTA pair
 
     // the swizzled operands need a 1024-byte aligned shared-memory window
     if (smem_u32(smem) & 1023u) {
@@ -437,37 +513,52 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
 
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
-            mbar_init(&full[i], kProducerWarps);  // one arrival per producer warp
+            // one arrival per producer warp, plus (kPair) one from CTA 1's forwarder
+            mbar_init(&full[i], kProducerWarps + (kCtas - 1));
             mbar_init(&empty[i], 1);
             mbar_init(&pdata[i], 1);
+            mbar_init(&sfree[i], kProducerWarps);
+            mbar_init(&pfull[i], kProducerWarps);
         }
         for (int i = 0; i < kBufs; ++i) {
             mbar_init(&acc_full[i], 1);
-            mbar_init(&acc_empty[i], kFlushWarps);  // one arrival per flush warp
+            mbar_init(&acc_empty[i], kFlushWarps * kCtas);  // one arrival per flush warp of the pair
         }
         mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32((const void*)tmem_slot)),
-                     "r"(kTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        // kPair: warp 0 of both CTAs allocates the same columns of both TMEMs
+        if constexpr (kCtas == 1) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32((const void*)tmem_slot)),
+                         "r"(kTmemCols)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32((const void*)tmem_slot)),
+                         "r"(kTmemCols)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        }
     }
     tc_fence_before();
-    __syncthreads();
+    if constexpr (kCtas == 1) __syncthreads();
+    else cluster_sync();  // both CTAs' barriers and TMEM are ready before any cross-CTA signal
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
         // ------------------------------------------------------------- MMA
-        if (lane == 0) {
+        // (kPair: CTA 0 issues the pair's MMAs; warp 0 of CTA 1 only
+        // allocates and releases TMEM)
+        if (lane == 0 && rank == 0) {
             int S = 0, C = 0;  // stages and chains issued so far by this CTA
-            for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
-                const TcItem I = tc_item<NMAX>(a, it);
-                const uint32_t idesc = mma_idesc(2 * I.nc);
+            for (int it = unit; it < a.n_items && !*abort_flag; it += n_units) {
+                const TcItem I = tc_item<MODE>(a, it, 0);
+                const uint32_t idesc = mma_idesc(kM * kCtas, 2 * I.nc);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
                     const int buf = S % kStages;
                     const int k = C + s / flush_stages;  // chain index
@@ -480,20 +571,40 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     const uint32_t base = smem_u32(smem + buf * kStageBytes);
                     const uint32_t a_hi = base, a_lo = base + kABytes;
                     const uint32_t b_hi = base + 2 * kABytes, b_lo = b_hi + SH::kBBytes;
-                    const uint32_t d = tmem + (uint32_t)(b * NMAX);
+                    const uint32_t d = tmem + (uint32_t)(b * SH::kN);
 #pragma unroll
                     for (int t = 0; t < kKr / 16; ++t) {
                         const uint32_t off = (uint32_t)(32 * t);
-                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc, (first && t == 0) ? 0u : 1u);
-                        mma_f16(d, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
-                        mma_f16(d, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, 1u);
+                        mma_f16<kCtas>(d, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc,
+                                       (first && t == 0) ? 0u : 1u);
+                        mma_f16<kCtas>(d, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
+                        mma_f16<kCtas>(d, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, 1u);
                     }
-                    mma_commit(&empty[buf]);
-                    if ((s % flush_stages) == flush_stages - 1 || s == I.n_stages - 1) mma_commit(&acc_full[b]);
+                    mma_commit<kCtas>(&empty[buf]);
+                    if ((s % flush_stages) == flush_stages - 1 || s == I.n_stages - 1) mma_commit<kCtas>(&acc_full[b]);
                 }
                 C += I.n_chunks;
             }
-            mma_commit(drain);
+            mma_commit<kCtas>(drain);
+        }
+        if constexpr (kCtas == 2) {
+            // CTA 1's forwarder: once all of this CTA's producer warps have
+            // filled a stage (local barrier), one cluster-scope arrival tells
+            // CTA 0, whose thread issues the pair's MMAs (one remote release per
+            // stage instead of one per producer warp)
+            if (lane == 0 && rank == 1) {
+                int S = 0;
+                for (int it = unit; it < a.n_items && !*abort_flag; it += n_units) {
+                    const TcItem I = tc_item<MODE>(a, it, 1);
+                    int s = 0;
+                    for (; s < I.n_stages; ++s, ++S) {
+                        const int buf = S % kStages;
+                        if (!mbar_wait(&pfull[buf], (S / kStages) & 1, abort_flag, a.error_flag, 256)) break;
+                        mbar_arrive_leader(&full[buf]);
+                    }
+                    if (s < I.n_stages) break;
+                }
+            }
         }
         __syncwarp();
     } else if (warp <= kFlushWarps) {
@@ -502,20 +613,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
         const int row = quarter * 32 + lane;  // M row owned by this thread
         int C = 0;
-        for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
-            const TcItem I = tc_item<NMAX>(a, it);
+        for (int it = unit; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += n_units) {
+            const TcItem I = tc_item<MODE>(a, it, rank);
             const size_t mk = (size_t)I.job->kx * I.job->ky;
             double* acc = I.job->acc;
             // the accumulator and the total hold 2^24 x the sum (units of the
             // operand scale); the exact 2^-24 is applied with W at the dump
             const double dump_scale = I.job->wmax * (double)kInvProductScale;
-            const int rho = I.m_tile * kM + row;
+            const int rho = I.row0 + row;
             const int c0 = I.c0;
             const int ncols = 2 * I.nc;
+            const int half_cols = 2 * I.bnc;  // columns from one CTA's B rows (all of them unless kPair)
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
                 const int b = k % kBufs, u = k / kBufs;
-                const uint32_t acc_col = lane_base + (uint32_t)(b * NMAX);
+                const uint32_t acc_col = lane_base + (uint32_t)(b * SH::kN);
                 // warp-uniform outcome: the warp arrives as one below
                 if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, 4))) break;
                 tc_fence_after();
@@ -549,13 +661,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     if (!dump) {
                         tmem_st32(lane_base + kColTotal + cc, tt);
                     } else {
-                        // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are contiguous
+                        // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are
+                        // contiguous.  Column n: CTA h = n / half_cols's B rows,
+                        // Re then Im of its bnc c values.
 #pragma unroll
                         for (int i = 0; i < 32; ++i) {
                             const int n = cc + i;
                             if (n < ncols) {
-                                const int im = n >= I.nc ? 1 : 0;
-                                const int c = c0 + n - im * I.nc;
+                                const int h = n / half_cols, nn = n - h * half_cols;
+                                const int im = nn >= I.bnc ? 1 : 0;
+                                const int c = c0 + h * I.bnc + nn - im * I.bnc;
                                 atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
                             }
                         }
@@ -563,7 +678,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&acc_empty[b]);
+                if (lane == 0) {
+                    // kPair: the accumulator release goes straight to CTA 0 (a
+                    // forwarding hop would lengthen the MMA's wait); CTA 0's
+                    // own warps arrive locally
+                    if (rank == 0) mbar_arrive(&acc_empty[b]);
+                    else mbar_arrive_leader(&acc_empty[b]);
+                }
             }
             C += I.n_chunks;
         }
@@ -572,13 +693,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         // ---------------------------------------------------------- loader
         if (lane == 0) {
             int S = 0;
-            for (int it = blockIdx.x; it < a.n_items && !*abort_flag; it += gridDim.x) {
-                const TcItem I = tc_item<NMAX>(a, it);
+            for (int it = unit; it < a.n_items && !*abort_flag; it += n_units) {
+                const TcItem I = tc_item<MODE>(a, it, rank);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
                     const int buf = S % kStages;
-                    // the producers are done with this slot once stage S - kStages is full
+                    // this CTA's producers have read the slot's constants of stage S - kStages
                     if (S >= kStages &&
-                        !mbar_wait(&full[buf], ((S / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
+                        !mbar_wait(&sfree[buf], ((S / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
                         break;
                     const int block = I.kb / kBlockParticles + s;
                     mbar_arrive_expect_tx(&pdata[buf], kBlockBytes);
@@ -596,11 +717,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         const int rc = (p >> 4) & 15;
         const int cb = (p >> 4) & 7;
         int S = 0;
-        for (int it = blockIdx.x; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += gridDim.x) {
-            const TcItem I = tc_item<NMAX>(a, it);
+        for (int it = unit; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += n_units) {
+            const TcItem I = tc_item<MODE>(a, it, rank);
             const int kx = I.job->kx, ky = I.job->ky;
             const bool gauss = I.job->gauss != 0;
-            const int rho0 = I.m_tile * kM + rc * 8;
+            const int rho0 = I.row0 + rc * 8;
             const int a_x = rho0 / ky - kx / 2;
             const int b0 = rho0 % ky - ky / 2;
             const bool a_up = b0 >= 0;
@@ -648,6 +769,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         pry[0] = pry[1] = make_float2(1.f, 0.f);
                     }
                 }
+                // the slot's constants are in registers: release it to the loader
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sfree[buf]);
                 if (!__all_sync(0xffffffffu,
                                 mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)))
                     break;
@@ -690,10 +814,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         else a_chain<false, false>(base, c16, X, Y, RX, RY, NRY, Q, RHO);
                     }
                 } else {
-                    // ---- B: c chunks cb and cb + 8 of the n-tile (8 c values each),
-                    // scaled by 2^12; rows [0, nc) hold (Re B, -Im B) pairs (the
-                    // Re F columns), rows [nc, 2 nc) (Im B, Re B) (the Im F columns).
-                    // Chunks at or beyond nc are not read by the MMA (N = 2 nc).
+                    // ---- B: c chunks cb (and cb + 8, kWide) of this CTA's bnc c values
+                    // from bc0 (8 each), scaled by 2^12; rows [0, bnc) hold (Re B, -Im B)
+                    // pairs (Re F columns), rows [bnc, 2 bnc) (Im B, Re B) (Im F columns).
+                    // Chunks at or beyond bnc are not read by the MMA.
                     uint8_t* bhi = st + 2 * kABytes;
                     RX = make_float2(prz[0].x, prz[1].x);
                     RY = make_float2(prz[0].y, prz[1].y);
@@ -702,8 +826,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
 #pragma unroll 1
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
-                        if (chunk * 8 >= I.nc) break;
-                        const int c_s = I.c0 + chunk * 8;
+                        if (chunk * 8 >= I.bnc) break;
+                        const int c_s = I.bc0 + chunk * 8;
                         float v[2][3];
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
@@ -722,7 +846,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         Y = make_float2(v[0][1], v[1][1]);
                         // nc and chunk * 8 are multiples of 8: row K of the chain is K within its atom
                         uint8_t* re_base = bhi + chunk * 8 * kRowBytes + (col & 15);
-                        uint8_t* im_base = bhi + (I.nc + chunk * 8) * kRowBytes + (col & 15);
+                        uint8_t* im_base = bhi + (I.bnc + chunk * 8) * kRowBytes + (col & 15);
                         const int c16 = col & ~15;
                         if (gauss) {
                             Q = make_float2(v[0][2], v[1][2]);
@@ -736,7 +860,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 // warp's lane 0 then arrives for the whole warp
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&full[buf]);
+                if (lane == 0) {
+                    // kPair: CTA 1's warps report to their forwarder (see the MMA role)
+                    if (rank == 0) mbar_arrive(&full[buf]);
+                    else mbar_arrive(&pfull[buf]);
+                }
             }
         }
     }
@@ -758,7 +886,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             }
         }
         __syncwarp();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        if constexpr (kCtas == 1)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                         : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                         : "memory");
+    }
+    // kPair: neither CTA exits while the other may still signal its barriers
+    if constexpr (kCtas == 2) {
+        __syncwarp();
+        cluster_sync();
     }
 }
 
@@ -853,6 +991,15 @@ bool is_spectrum_lattice(const Lattice& L) {
 
 // Stages per TMEM accumulation chain before a flush into the FP32 total:
 // MV_TC_FLUSH_STAGES (1..1024) overrides the tuned (or default) value.
+// kPair tiles: MV_TC_PAIRS=0 turns them off (jobs then take kWide tiles).
+bool tc_pairs_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("MV_TC_PAIRS");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
 int tc_flush_stages() {
     static const int env = [] {
         const char* e = std::getenv("MV_TC_FLUSH_STAGES");
@@ -896,9 +1043,10 @@ struct ClassKey {
 int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     plan = TensorPlan{};
     std::vector<ClassKey> keys;
-    // (narrow tile?, stages, item): NMAX = 128 items first, each kind longest first
+    // (tile mode, cost, item): kNarrow items first, then kPair, then kWide;
+    // each mode longest first
     struct Item {
-        int wide;
+        int mode;
         long long cost;
         int2 item;
     };
@@ -944,22 +1092,29 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.kx = kx;
         j.ky = ky;
         j.lz_tc = lz_tc;
-        const int wide = lz_tc > Shape<128>::kNc ? 1 : 0;  // NMAX = 256 beyond 64 tensor planes
-        // equal n-tiles of at most NMAX / 2 c values: 192 planes -> 96 + 96
-        // (two N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by
-        // its shared-memory operand reads)
-        const int nc_max = wide ? Shape<256>::kNc : Shape<128>::kNc;
+        // tile mode: kNarrow up to 64 tensor planes; beyond, kPair where every
+        // n-tile splits into two halves of 8-c chunks and the rows into
+        // 256-row m-tiles, else kWide
+        const int mode = lz_tc <= Shape<kNarrow>::kNc                                         ? kNarrow
+                         : (tc_pairs_enabled() && lz_tc % 16 == 0 && ((long long)kx * ky) % 256 == 0) ? kPair
+                                                                                                    : kWide;
+        // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
+        // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
+        // shared-memory operand reads); multiples of 16 for kPair
+        const int nc_max = mode == kNarrow ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
+        const int nc_unit = mode == kPair ? 16 : 8;
         j.n_ntiles = (lz_tc + nc_max - 1) / nc_max;
-        j.nc_tile = ((lz_tc + j.n_ntiles - 1) / j.n_ntiles + 7) / 8 * 8;
+        j.nc_tile = ((lz_tc + j.n_ntiles - 1) / j.n_ntiles + nc_unit - 1) / nc_unit * nc_unit;
         j.n_ntiles = (lz_tc + j.nc_tile - 1) / j.nc_tile;
-        j.n_mtiles = (int)((long long)kx * ky / kM);
+        const int ctas = mode == kPair ? 2 : 1;
+        j.n_mtiles = (int)((long long)kx * ky / (kM * ctas));
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
         // particle splits: enough items per group for ~tc_waves waves on its
         // own (default 4), at least 64 stages each
         const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
-        const long long target = (long long)device_sm_count() * active_tune().tc_waves;
+        const long long target = (long long)(device_sm_count() / ctas) * active_tune().tc_waves;
         long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
         splits = std::min<long long>(splits, std::max<long long>(1, (r.n + 64 * kKp - 1) / (64 * kKp)));
         const long long chunk = ((r.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
@@ -972,19 +1127,21 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(r.n, k0 + chunk);
             const long long stages = (k1 - k0 + kKp - 1) / kKp;
             for (long long t = 0; t < ftiles; ++t)
-                items.push_back({wide, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+                items.push_back({mode, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
         }
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
-    // per tile width, longest first (round-robin over the persistent CTAs)
-    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) {
-        return x.wide != y.wide ? x.wide < y.wide : x.cost > y.cost;
+    // per tile mode, longest first (round-robin over the persistent CTAs / pairs)
+    auto order = [](int m) { return m == kNarrow ? 0 : m == kPair ? 1 : 2; };
+    std::stable_sort(items.begin(), items.end(), [&](const Item& x, const Item& y) {
+        return x.mode != y.mode ? order(x.mode) < order(y.mode) : x.cost > y.cost;
     });
     plan.items.reserve(items.size());
-    plan.n_narrow = 0;
+    plan.n_narrow = plan.n_pair = 0;
     for (auto& it : items) {
         plan.items.push_back(it.item);
-        plan.n_narrow += it.wide ? 0 : 1;
+        plan.n_narrow += it.mode == kNarrow ? 1 : 0;
+        plan.n_pair += it.mode == kPair ? 1 : 0;
     }
     plan.meta_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256 + plan.items.size() * sizeof(int2);
     return kOk;
@@ -1050,30 +1207,62 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
     }
     st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
     if (st != kOk) return st;
-    // one persistent launch per tile width for all groups
+    // one persistent launch per tile mode for all groups
     if (!plan.items.empty()) {
         timer_begin(timer, 3, stream);
-        for (int wide = 0; wide < 2 && st == kOk; ++wide) {
+        const int counts[3] = {plan.n_narrow, plan.n_pair, (int)plan.items.size() - plan.n_narrow - plan.n_pair};
+        int first = 0;
+        for (int m = 0; m < 3 && st == kOk; first += counts[m], ++m) {
             TcArgs a;
             a.jobs = static_cast<const TcJob*>(plan.d_jobs);
-            a.items = static_cast<const int2*>(plan.d_items) + (wide ? plan.n_narrow : 0);
-            a.n_items = wide ? (int)plan.items.size() - plan.n_narrow : plan.n_narrow;
+            a.items = static_cast<const int2*>(plan.d_items) + first;
+            a.n_items = counts[m];
             a.flush_stages = plan.flush;
             a.error_flag = error_flag;
             if (a.n_items == 0) continue;
-            const int grid = std::min<int>(a.n_items, device_sm_count());
-            if (wide) {
-                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)Shape<256>::kSmemBytes),
+            if (m == 0) {
+                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kNarrow>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)Shape<kNarrow>::kSmemBytes),
                                 "cudaFuncSetAttribute");
                 if (st != kOk) break;
-                tc_sum_kernel<256><<<grid, kThreads, Shape<256>::kSmemBytes, stream>>>(a);
+                const int grid = std::min<int>(a.n_items, device_sm_count());
+                tc_sum_kernel<kNarrow><<<grid, kThreads, Shape<kNarrow>::kSmemBytes, stream>>>(a);
+            } else if (m == 2) {
+                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)Shape<kWide>::kSmemBytes),
+                                "cudaFuncSetAttribute");
+                if (st != kOk) break;
+                const int grid = std::min<int>(a.n_items, device_sm_count());
+                tc_sum_kernel<kWide><<<grid, kThreads, Shape<kWide>::kSmemBytes, stream>>>(a);
             } else {
-                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)Shape<128>::kSmemBytes),
+                // CTA pairs: clusters of 2, as many as can be resident at once
+                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kPair>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)Shape<kPair>::kSmemBytes),
                                 "cudaFuncSetAttribute");
                 if (st != kOk) break;
-                tc_sum_kernel<128><<<grid, kThreads, Shape<128>::kSmemBytes, stream>>>(a);
+                cudaLaunchConfig_t lc = {};
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = 2;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                lc.blockDim = dim3(kThreads);
+                lc.dynamicSmemBytes = Shape<kPair>::kSmemBytes;
+                lc.stream = stream;
+                lc.attrs = attr;
+                lc.numAttrs = 1;
+                lc.gridDim = dim3(2 * std::max(1, device_sm_count() / 2));
+                int clusters = 0;
+                st = check_cuda(cudaOccupancyMaxActiveClusters(&clusters, tc_sum_kernel<kPair>, &lc),
+                                "cudaOccupancyMaxActiveClusters");
+                if (st != kOk) break;
+                if (clusters < 1) {
+                    st = set_error(kCudaError, "tensor sum: no CTA pair fits on this device");
+                    break;
+                }
+                lc.gridDim = dim3(2 * std::min(a.n_items, clusters));
+                st = check_cuda(cudaLaunchKernelEx(&lc, tc_sum_kernel<kPair>, a), "tc_sum_kernel (pairs) launch");
+                if (st != kOk) break;
             }
             count_launch();
             st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");

@@ -262,11 +262,12 @@ def test_tensor_form_matches_fp64(case):
 
 
 @pytest.mark.parametrize("case", ["gauss_decaying_radii", "wendland_uniform_radius"])
-@pytest.mark.parametrize("grid", [(32, 32, 272), (32, 32, 16)])
+@pytest.mark.parametrize("grid", [(32, 32, 272), (32, 32, 288), (32, 32, 16)])
 def test_tensor_form_uneven_and_narrowest_n_tiles(case, grid):
     """32x32x272: the tensor planes c < 136 split into n-tiles of 72 and 64 c
-    values (MMA N = 144 and 128); 32x32x16: one tile of 8 (N = 16, the
-    smallest MMA width)."""
+    values (one CTA, MMA N = 144 and 128); 32x32x288: 144 planes, a multiple
+    of 16, go to CTA pairs with n-tiles of 80 and 64 c values (40 and 32 per
+    CTA); 32x32x16: one tile of 8 (N = 16, the smallest MMA width)."""
     rng = np.random.default_rng(23)
     groups = _tc_groups(rng, 2001)[case]
     spec, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
