@@ -100,8 +100,9 @@ int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int 
 /* Picks the launch parameters of vis_spectrum_compute for this spectrum's
  * shape (lattice, total particles of the dataset, number of groups, form) by
  * timing candidates on the caller's data: the plain form's split-K (2, 4, 6, 8
- * blocks per SM), the tensor form's particle splits (2, 4, 8 waves) and its
- * accumulation chain (4 or 8 stages; longer chains lose accuracy).  Each
+ * blocks per SM), the tensor form's particle splits (2, 4, 8 waves) and the
+ * accumulation chain of its single-accumulator tiles (8 or 16 stages; longer
+ * chains lose accuracy; the double-buffered tile keeps at most 8).  Each
  * candidate runs vis_spectrum_compute twice (the spectrum holds the last
  * result); the best set is kept for the process and used by later computes of
  * the same shape.  best_ms (may be NULL) receives its time.  No counterpart in
@@ -110,7 +111,7 @@ int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int 
 int vis_autotune_spectrum(VisSpectrum* spectrum, VisConfig* vis_config, MeshlessDataset* meshless_dataset, int form,
                           float* best_ms);
 /* The parameters that computes of this shape use; returns 1 if they were
- * tuned, 0 for the defaults (6, 4, 8). */
+ * tuned, 0 for the defaults (6, 4, 16). */
 int vis_autotune_lookup(int3 grid_size, long long number_of_terms, int number_of_groups, int form,
                         int* plain_waves, int* tensor_waves, int* tensor_flush_stages);
 void vis_autotune_clear(void);

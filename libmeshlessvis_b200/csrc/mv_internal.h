@@ -162,7 +162,8 @@ struct TensorPlan {
     size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
     const void* d_jobs = nullptr;
     const void* d_items = nullptr;
-    int flush = 8;  // stages per TMEM accumulation chain, as planned
+    int flush = 16;        // stages per TMEM accumulation chain of the kWide / kPair tiles, as planned
+    int flush_narrow = 8;  // the same for the kNarrow tile
 };
 
 struct TensorWorkspace {
@@ -197,7 +198,8 @@ int device_sm_count();
 struct TuneParams {
     int plain_waves = 6;  // plain form: split-K until the grid holds ~plain_waves blocks per SM
     int tc_waves = 4;     // tensor form: particle splits until the items make ~tc_waves waves
-    int tc_flush = 8;     // tensor form: stages per TMEM accumulation chain (4 or 8)
+    int tc_flush = 16;    // tensor form, single-accumulator tiles: stages per TMEM chain (8 or 16;
+                          // the double-buffered 128x128 tile uses at most 8)
 };
 // The parameters in force on this thread: set by TuneScope around a compute.
 const TuneParams& active_tune();

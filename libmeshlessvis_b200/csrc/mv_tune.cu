@@ -2,8 +2,9 @@
 // kernels otherwise derive from fixed rules (TuneParams in mv_internal.h):
 //   plain_waves  split-K of the plain form, in blocks per SM: 2, 4, 6, 8
 //   tc_waves     particle splits of the tensor form, in waves: 2, 4, 8
-//   tc_flush     tensor-core accumulation chain, in stages: 4, 8 (longer
-//                chains lose accuracy, so they are not candidates)
+//   tc_flush     tensor-core accumulation chain of the single-accumulator
+//                tiles, in stages: 8, 16 (longer chains lose accuracy, so
+//                they are not candidates)
 // vis_autotune_spectrum times each candidate on the caller's own data through
 // the public compute path (one warm-up and one timed run, CUDA events on the
 // config's stream), one parameter at a time starting from the defaults, and
@@ -86,7 +87,7 @@ int vis_autotune_spectrum(VisSpectrum* sp, VisConfig* vis_config, MeshlessDatase
     };
     TuneParams best;
     float best_t = time_of(best);
-    const int plain_c[] = {2, 4, 6, 8}, waves_c[] = {2, 4, 8}, flush_c[] = {8, 4};
+    const int plain_c[] = {2, 4, 6, 8}, waves_c[] = {2, 4, 8}, flush_c[] = {16, 8};
     for (int field = 0; field < 3 && best_t >= 0.f; ++field) {
         const int* cand = field == 0 ? plain_c : field == 1 ? waves_c : flush_c;
         const int count = field == 0 ? 4 : field == 1 ? 3 : 2;

@@ -175,10 +175,11 @@ def test_write_ppm_layout_and_flip(tmp_path):
 
 def test_autotune_table_starts_with_the_defaults():
     """Without a tuning run, every shape reports the default launch parameters
-    (plain split-K 6 blocks per SM, tensor splits 4 waves, 8-stage chains)."""
+    (plain split-K 6 blocks per SM, tensor splits 4 waves, 16-stage chains
+    in the single-accumulator tiles)."""
     lib = L.load()
     lib.vis_autotune_clear()
     vals = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
     tuned = lib.vis_autotune_lookup(L.int3(64, 64, 64), 4096, 2, 0, *[ctypes.byref(v) for v in vals])
     assert tuned == 0
-    assert [v.value for v in vals] == [6, 4, 8]
+    assert [v.value for v in vals] == [6, 4, 16]
