@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
 #pragma unroll
             for (int i = 0; i < NP; ++i) acc[m][i] = make_float2(0.f, 0.f);
 
-#pragma unroll 1
+#pragma unroll 2
         for (int j = 0; j < cnt; ++j) {
             const uint4 q = s_q[j];
             const float2 R = s_rot[j];
