@@ -119,27 +119,40 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 //   tensor_reserve_upload grows the workspaces and uploads the job and item
 //                         tables (not capturable in a CUDA graph);
 //   tensor_enqueue        memsets, per-particle constants, the persistent
-//                         launch, FP64 -> spectrum (added), Nyquist planes
-//                         (plain form, added); stream-ordered and capturable
-//                         once the workspaces are large enough.
+//                         launch, FP64 -> spectrum (added), the Nyquist planes
+//                         of groups without a Nyquist job (plain form, added);
+//                         stream-ordered and capturable once the workspaces
+//                         are large enough.
 // The spectra must be zeroed (or hold earlier groups) before tensor_enqueue.
 int tensor_sum_available(const SumRequest& req);
 
 // One job of the persistent tensor-core kernel: a separable group summed over
-// a half-spectrum lattice into an FP64 accumulator.  Its work items are
-// (split ks, m tile, n tile), local index (ks * n_mtiles + m_tile) * n_ntiles
-// + n_tile.  Device-resident (64 bytes).
+// a lattice of rows (a, b) and columns c >= 0 into an FP64 accumulator.  Its
+// work items are (split ks, m tile, n tile), local index (ks * n_mtiles +
+// m_tile) * n_ntiles + n_tile.  Device-resident (72 bytes).
+//
+// Frequencies: a = a_idx + a_base, b = b_idx + b_base, c = c_idx + c_base.
+// A group's planes c < Kz/2 are one job (a_base = -Kx/2, b_base = -Ky/2,
+// c_base = 0).  Its Nyquist plane c = Kz/2 is two transposed jobs over the
+// same particles with x and z exchanged, so that their one row index a_idx = 0
+// carries the frequency of z and their columns the frequencies of x:
+//   a >= 0: a_base = Kz/2, rows b (b_base = -Ky/2), columns 0 .. Kx/2 - 1;
+//   a < 0:  F(a, b, Kz/2) = conj F(-a, -b, -Kz/2), so a_base = -Kz/2, rows
+//           b' = -b (b_base = 1 - Ky/2), columns -a = 1 .. Kx/2 (c_base = 1).
+// Every column frequency is >= 0: the B chains only rise.
 struct TcJob {
     const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
-    double* acc;           // [c][Re, Im][a_idx * ky + b_idx]
+    double* acc;           // [c_idx][Re, Im][a_idx * ky + b_idx]
     double wmax;
-    int kx, ky, lz_tc;  // lattice extents; c planes [0, lz_tc) are summed here
+    int kx, ky, lz_tc;  // row extents (a_idx < kx, b_idx < ky); columns c_idx < lz_tc
     int n_mtiles, n_ntiles;
     int n;        // particles
     int k_chunk;  // particles per item (multiple of 32)
     int gauss;    // per-particle Gaussian factors (GAUSSIAN_DECAYING with radii)
     int nc_tile;  // c values per n-tile (a multiple of 8; the last tile may be narrower)
-    int pad;
+    int a_base;   // frequency of row index a_idx = 0
+    int b_base;   // frequency of row index b_idx = 0 (-Ky/2 or 1 - Ky/2: 8-row chunks never hold both signs)
+    int c_base;   // frequency of column c_idx = 0 (>= 0)
 };
 
 struct TensorPlan {
@@ -152,13 +165,16 @@ struct TensorPlan {
         bool factored;
         double scale;
         size_t acc_offset;
+        bool nyquist;             // the Nyquist plane is summed by the groups' transposed jobs
+        size_t acc_nyq_offset;    // their FP64 accumulator: the a < 0 job's columns, then the a >= 0 job's
     };
     std::vector<TcJob> jobs;
     std::vector<int2> items;  // 128x128-tile items (n_narrow), CTA-pair items (n_pair), then 128x256
     int n_narrow = 0, n_pair = 0;
     std::vector<Class> classes;
     std::vector<int> group_class, job_of_group;
-    std::vector<size_t> tp_offset;
+    std::vector<int> nyq_job_of_group;  // the transposed Nyquist-plane jobs (a >= 0 here, a < 0 next), or -1
+    std::vector<size_t> tp_offset, tp_nyq_offset;
     size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
     const void* d_jobs = nullptr;
     const void* d_items = nullptr;

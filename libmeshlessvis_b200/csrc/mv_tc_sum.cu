@@ -31,6 +31,12 @@
 // so a warp's rows are contiguous), which a finalize kernel converts to the
 // float2 spectrum.
 //
+// The Nyquist plane c = Kz/2 is the same kind of GEMM with the axes
+// exchanged: rows b with the fixed frequency Kz/2 on z, columns a on x (two
+// jobs, a >= 0 and, by F(-a, b, c) = conj F(a, -b, -c), a < 0; see TcJob), so
+// it runs as 1/Kx of the other planes' tiles in the same launch instead of a
+// plain-form pass.
+//
 // CTA tile: M = 128 rows (a, b) (8-row chunks of constant a), N = up to 128 c
 // values (256 real columns: the 128x256 MMA reads A once for twice the work of
 // a 128x128 one, within the shared-memory port), K = 32 particles (64 real)
@@ -163,6 +169,7 @@ struct TcItem {
     int c0, nc;    // the n-tile's first c and c values (a multiple of 8); the MMA's N is 2 nc
     int bc0, bnc;  // the c values whose B rows this CTA produces: all of them, or one half (kPair)
     int row0;      // this CTA's first lattice row
+    int a_base, b_base, c_base;  // the job's frequency offsets, in registers for the stage loops
 };
 
 template <int MODE>
@@ -184,6 +191,9 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.bnc = r.nc / Shape<MODE>::kCtas;
     r.bc0 = r.c0 + rank * r.bnc;
     r.row0 = r.m_tile * Shape<MODE>::kMTile + rank * kM;
+    r.a_base = r.job->a_base;
+    r.b_base = r.job->b_base;
+    r.c_base = r.job->c_base;
     return r;
 }
 
@@ -719,11 +729,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         int S = 0;
         for (int it = unit; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += n_units) {
             const TcItem I = tc_item<MODE>(a, it, rank);
-            const int kx = I.job->kx, ky = I.job->ky;
+            const int ky = I.job->ky;
             const bool gauss = I.job->gauss != 0;
             const int rho0 = I.row0 + rc * 8;
-            const int a_x = rho0 / ky - kx / 2;
-            const int b0 = rho0 % ky - ky / 2;
+            const int a_x = rho0 / ky + I.a_base;
+            const int b0 = rho0 % ky + I.b_base;
             const bool a_up = b0 >= 0;
             const int b_s = a_up ? b0 : b0 + 7;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
@@ -827,7 +837,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.bnc) break;
-                        const int c_s = I.bc0 + chunk * 8;
+                        const int c_s = I.bc0 + chunk * 8 + I.c_base;  // >= 0: the chain rises
                         float v[2][3];
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
@@ -908,7 +918,8 @@ struct TcPrepArgs {
     float gamma_scale;
     float inv_wmax;
     bool gauss;
-    uint8_t* out;  // ceil(n / 32) blocks
+    uint8_t* out;      // ceil(n / 32) blocks
+    uint8_t* out_nyq;  // the same with x and z exchanged (the Nyquist-plane job's), or null
 };
 
 __global__ void tc_prep_kernel(TcPrepArgs p) {
@@ -936,12 +947,28 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
     reinterpret_cast<float*>(blk + kOffAmp)[l] = amp;
     reinterpret_cast<float*>(blk + kOffGam)[l] = gam;
     reinterpret_cast<float*>(blk + kOffRho2)[l] = exp2f(2.f * gam);
-    reinterpret_cast<float2*>(blk + kOffRy)[l] = unit_phase(qy);
+    const float2 ry = unit_phase(qy);
+    reinterpret_cast<float2*>(blk + kOffRy)[l] = ry;
     reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(qz);
+    if (p.out_nyq) {
+        uint8_t* t = p.out_nyq + (size_t)(j / kBlockParticles) * kBlockBytes;
+        reinterpret_cast<uint32_t*>(t + kOffQx)[l] = qz;
+        reinterpret_cast<uint32_t*>(t + kOffQy)[l] = qy;
+        reinterpret_cast<uint32_t*>(t + kOffQz)[l] = qx;
+        reinterpret_cast<float*>(t + kOffAmp)[l] = amp;
+        reinterpret_cast<float*>(t + kOffGam)[l] = gam;
+        reinterpret_cast<float*>(t + kOffRho2)[l] = exp2f(2.f * gam);
+        reinterpret_cast<float2*>(t + kOffRy)[l] = ry;
+        reinterpret_cast<float2*>(t + kOffRz)[l] = unit_phase(qx);
+    }
 }
 
 // acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
 // Phi^ factor (groups whose Phi^ factors out) and the scale, written or added.
+// nyquist: the plane c = lz_tc alone, from the transposed jobs' accumulator
+// [column][Re, Im][row]: for a >= 0, column a + Kx/2 and row b + Ky/2; for a <
+// 0 the conjugate of column -a - 1 (frequency -a) at row Ky/2 - 1 - b
+// (frequency -b).
 struct TcFinalizeArgs {
     const double* acc;
     int kx, ky, lz_tc, lz_out;
@@ -952,14 +979,16 @@ struct TcFinalizeArgs {
     double scale;
     float2* out;
     bool accumulate;
+    bool nyquist;
 };
 
 __global__ void tc_finalize_kernel(TcFinalizeArgs f) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long count = (long long)f.kx * f.ky * f.lz_tc;
+    const int planes = f.nyquist ? 1 : f.lz_tc;
+    const long long count = (long long)f.kx * f.ky * planes;
     if (q >= count) return;
-    const int c = (int)(q % f.lz_tc);
-    const long long rho = q / f.lz_tc;
+    const int c = f.nyquist ? f.lz_tc : (int)(q % f.lz_tc);
+    const long long rho = q / planes;
     const int b = (int)(rho % f.ky) - f.ky / 2;
     const int a = (int)(rho / f.ky) - f.kx / 2;
     double factor = f.scale;
@@ -967,10 +996,25 @@ __global__ void tc_finalize_kernel(TcFinalizeArgs f) {
         const double k = f.step * sqrt((double)a * a + (double)b * b + (double)c * c);
         factor *= phi_fp64(f.basis, k * f.h);
     }
-    // accumulator layout [c][Re, Im][row]
-    const size_t mk = (size_t)f.kx * f.ky;
-    const float re = (float)(f.acc[(size_t)(2 * c) * mk + rho] * factor);
-    const float im = (float)(f.acc[(size_t)(2 * c + 1) * mk + rho] * factor);
+    size_t i_re, i_im;
+    double conj = 1.0;
+    if (f.nyquist) {
+        const int a_idx = (int)(rho / f.ky), b_idx = (int)(rho % f.ky);
+        if (a >= 0) {
+            i_re = (size_t)(2 * a_idx) * f.ky + b_idx;
+        } else {
+            i_re = (size_t)(2 * (-a - 1)) * f.ky + (f.ky - 1 - b_idx);
+            conj = -1.0;
+        }
+        i_im = i_re + f.ky;
+    } else {
+        // accumulator layout [c][Re, Im][row]
+        const size_t mk = (size_t)f.kx * f.ky;
+        i_re = (size_t)(2 * c) * mk + rho;
+        i_im = i_re + mk;
+    }
+    const float re = (float)(f.acc[i_re] * factor);
+    const float im = (float)(f.acc[i_im] * factor * conj);
     const size_t idx = (size_t)rho * f.lz_out + c;
     if (f.accumulate) {
         const float2 o = f.out[idx];
@@ -1018,7 +1062,7 @@ int tc_flush_stages(int mode) {
 int tensor_sum_available(const SumRequest& r) {
     const Lattice& L = r.lat;
     if (!is_spectrum_lattice(L) || r.wrap != 0) return 0;
-    const int lz_tc = L.nz - 1;  // planes [0, Kz/2); the Nyquist plane goes to the plain form
+    const int lz_tc = L.nz - 1;  // planes [0, Kz/2); the Nyquist plane is planned separately
     if (L.ny % 16 || ((long long)L.nx * L.ny) % kM || lz_tc % 8 || lz_tc < 8) return 0;
     if ((long long)L.nx * L.ny * lz_tc * 2 > (1LL << 31)) return 0;
     if (r.weight_max < 0.f) return 0;  // needs the registered |weight| maximum
@@ -1057,6 +1101,39 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     std::vector<Item> items;
     plan.flush_narrow = tc_flush_stages(kNarrow);
     plan.flush = tc_flush_stages(kWide);
+    // Tiles and particle splits of a job (rows kx * ky, columns lz_tc), its
+    // items appended; returns the job's index.
+    auto add_job = [&](TcJob j, int mode) {
+        // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
+        // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
+        // shared-memory operand reads); multiples of 16 for kPair
+        const int nc_max = mode == kNarrow ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
+        const int nc_unit = mode == kPair ? 16 : 8;
+        j.n_ntiles = (j.lz_tc + nc_max - 1) / nc_max;
+        j.nc_tile = ((j.lz_tc + j.n_ntiles - 1) / j.n_ntiles + nc_unit - 1) / nc_unit * nc_unit;
+        j.n_ntiles = (j.lz_tc + j.nc_tile - 1) / j.nc_tile;
+        const int ctas = mode == kPair ? 2 : 1;
+        j.n_mtiles = (int)((long long)j.kx * j.ky / (kM * ctas));
+        // particle splits: enough items per job for ~tc_waves waves on its
+        // own (default 4), at least 64 stages each
+        const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
+        const long long target = (long long)(device_sm_count() / ctas) * active_tune().tc_waves;
+        long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
+        splits = std::min<long long>(splits, std::max<long long>(1, (j.n + 64 * kKp - 1) / (64 * kKp)));
+        const long long chunk = ((j.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
+        splits = (j.n + chunk - 1) / chunk;
+        j.k_chunk = (int)chunk;
+        const int job_index = (int)plan.jobs.size();
+        plan.jobs.push_back(j);
+        const int flush = mode == kNarrow ? plan.flush_narrow : plan.flush;
+        for (long long ks = 0; ks < splits; ++ks) {
+            const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
+            const long long stages = (k1 - k0 + kKp - 1) / kKp;
+            for (long long t = 0; t < ftiles; ++t)
+                items.push_back({mode, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+        }
+        return job_index;
+    };
     for (size_t g = 0; g < groups.size(); ++g) {
         const SumRequest& r = groups[g];
         const Lattice& L = r.lat;
@@ -1083,56 +1160,65 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             c.scale = r.scale;
             c.acc_offset = plan.acc_bytes;
             plan.acc_bytes += ((size_t)kx * ky * lz_tc * 2 * sizeof(double) + 255) / 256 * 256;
+            c.nyquist = false;
+            c.acc_nyq_offset = 0;
             plan.classes.push_back(c);
         }
         plan.group_class.push_back(cls);
+        const size_t blocks_bytes =
+            (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
         plan.tp_offset.push_back(plan.tp_bytes);
-        plan.tp_bytes += (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
+        plan.tp_bytes += blocks_bytes;
+        plan.tp_nyq_offset.push_back(0);
+        plan.nyq_job_of_group.push_back(-1);
         if (r.n <= 0 || !(r.weight_max > 0.f)) {
             plan.job_of_group.push_back(-1);
             continue;
         }
-        TcJob j{};
-        j.kx = kx;
-        j.ky = ky;
-        j.lz_tc = lz_tc;
         // tile mode: kNarrow up to 64 tensor planes; beyond, kPair where every
         // n-tile splits into two halves of 8-c chunks and the rows into
         // 256-row m-tiles, else kWide
         const int mode = lz_tc <= Shape<kNarrow>::kNc                                         ? kNarrow
                          : (tc_pairs_enabled() && lz_tc % 16 == 0 && ((long long)kx * ky) % 256 == 0) ? kPair
                                                                                                     : kWide;
-        // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
-        // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
-        // shared-memory operand reads); multiples of 16 for kPair
-        const int nc_max = mode == kNarrow ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
-        const int nc_unit = mode == kPair ? 16 : 8;
-        j.n_ntiles = (lz_tc + nc_max - 1) / nc_max;
-        j.nc_tile = ((lz_tc + j.n_ntiles - 1) / j.n_ntiles + nc_unit - 1) / nc_unit * nc_unit;
-        j.n_ntiles = (lz_tc + j.nc_tile - 1) / j.nc_tile;
-        const int ctas = mode == kPair ? 2 : 1;
-        j.n_mtiles = (int)((long long)kx * ky / (kM * ctas));
+        TcJob j{};
+        j.kx = kx;
+        j.ky = ky;
+        j.lz_tc = lz_tc;
+        j.a_base = -kx / 2;
+        j.b_base = -ky / 2;
+        j.c_base = 0;
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
-        // particle splits: enough items per group for ~tc_waves waves on its
-        // own (default 4), at least 64 stages each
-        const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
-        const long long target = (long long)(device_sm_count() / ctas) * active_tune().tc_waves;
-        long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
-        splits = std::min<long long>(splits, std::max<long long>(1, (r.n + 64 * kKp - 1) / (64 * kKp)));
-        const long long chunk = ((r.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
-        splits = (r.n + chunk - 1) / chunk;
-        j.k_chunk = (int)chunk;
-        const int job_index = (int)plan.jobs.size();
-        plan.job_of_group.push_back(job_index);
-        plan.jobs.push_back(j);
-        for (long long ks = 0; ks < splits; ++ks) {
-            const long long k0 = ks * chunk, k1 = std::min<long long>(r.n, k0 + chunk);
-            const long long stages = (k1 - k0 + kKp - 1) / kKp;
-            const int flush = mode == kNarrow ? plan.flush_narrow : plan.flush;
-            for (long long t = 0; t < ftiles; ++t)
-                items.push_back({mode, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+        plan.job_of_group.push_back(add_job(j, mode));
+        // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
+        // -a > 0; see TcJob) in the same launch, where its Ky rows fill whole
+        // m-tiles of the group's tile mode and its Kx / 2 columns per job split
+        // into whole n-tile units (16 c for kPair, else 8); otherwise the
+        // plain form sums it.
+        const int ctas = mode == kPair ? 2 : 1;
+        if (ky % (kM * ctas) == 0 && (kx / 2) % (mode == kPair ? 16 : 8) == 0 && kx % 2 == 0) {
+            TcJob t = j;
+            t.kx = 1;
+            t.ky = ky;
+            t.lz_tc = kx / 2;
+            t.a_base = lz_tc;
+            t.b_base = -ky / 2;
+            t.c_base = 0;
+            plan.nyq_job_of_group.back() = add_job(t, mode);
+            t.a_base = -lz_tc;
+            t.b_base = 1 - ky / 2;
+            t.c_base = 1;
+            add_job(t, mode);
+            plan.tp_nyq_offset.back() = plan.tp_bytes;
+            plan.tp_bytes += blocks_bytes;
+            TensorPlan::Class& c = plan.classes[cls];
+            if (!c.nyquist) {
+                c.nyquist = true;
+                c.acc_nyq_offset = plan.acc_bytes;
+                plan.acc_bytes += ((size_t)kx * ky * 2 * sizeof(double) + 255) / 256 * 256;
+            }
         }
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
@@ -1162,8 +1248,18 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     for (size_t g = 0; g < plan.job_of_group.size(); ++g) {
         const int j = plan.job_of_group[g];
         if (j < 0) continue;
+        const TensorPlan::Class& c = plan.classes[plan.group_class[g]];
         plan.jobs[j].blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.tp_offset[g]);
-        plan.jobs[j].acc = reinterpret_cast<double*>(acc_base + plan.classes[plan.group_class[g]].acc_offset);
+        plan.jobs[j].acc = reinterpret_cast<double*>(acc_base + c.acc_offset);
+        const int t = plan.nyq_job_of_group[g];
+        if (t < 0) continue;
+        // both Nyquist jobs read the same transposed constants; the a < 0
+        // job's Kx/2 columns come first in the accumulator, then the a >= 0 job's
+        double* nyq_acc = reinterpret_cast<double*>(acc_base + c.acc_nyq_offset);
+        plan.jobs[t].blocks = plan.jobs[t + 1].blocks =
+            reinterpret_cast<const unsigned char*>(tp_base + plan.tp_nyq_offset[g]);
+        plan.jobs[t].acc = nyq_acc + (size_t)(c.kx / 2) * 2 * c.ky;
+        plan.jobs[t + 1].acc = nyq_acc;
     }
     std::vector<char> meta(plan.meta_bytes, 0);
     const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
@@ -1207,6 +1303,8 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         pa.gamma_scale = pa.gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
         pa.inv_wmax = 1.0f / r.weight_max;
         pa.out = const_cast<unsigned char*>(plan.jobs[j].blocks);
+        const int t = plan.nyq_job_of_group[g];
+        pa.out_nyq = t < 0 ? nullptr : const_cast<unsigned char*>(plan.jobs[t].blocks);
         tc_prep_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(pa);
         count_launch();
     }
@@ -1290,14 +1388,25 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         f.scale = c.scale;
         f.out = c.out;
         f.accumulate = true;
+        f.nyquist = false;
         const long long count = (long long)c.kx * c.ky * c.lz_tc;
         tc_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(f);
         count_launch();
+        if (c.nyquist) {
+            f.acc = reinterpret_cast<const double*>(static_cast<const char*>(ws.acc.ptr) + c.acc_nyq_offset);
+            f.nyquist = true;
+            const long long plane = (long long)c.kx * c.ky;
+            tc_finalize_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, stream>>>(f);
+            count_launch();
+        }
     }
     st = check_cuda(cudaGetLastError(), "tc_finalize_kernel launch");
     if (st != kOk) return st;
-    // the Nyquist plane l = Kz/2 of every group with the plain form
-    for (const SumRequest& r : groups) {
+    // the Nyquist plane l = Kz/2 with the plain form, for groups without a
+    // transposed job (groups without particles or weight have neither)
+    for (size_t g = 0; g < groups.size(); ++g) {
+        if (plan.job_of_group[g] >= 0 && plan.nyq_job_of_group[g] >= 0) continue;
+        const SumRequest& r = groups[g];
         SumRequest nyq = r;
         const int lz_tc = r.lat.nz - 1;
         nyq.lat.z0 = lz_tc;

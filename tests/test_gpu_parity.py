@@ -277,6 +277,29 @@ def test_tensor_form_uneven_and_narrowest_n_tiles(case, grid):
     assert O.rel_l2(spec[:, :, lz - 8:lz], ref[:, :, lz - 8:lz]) < SPEC_TOL  # the last tile's planes
 
 
+@pytest.mark.parametrize("case", ["gauss_decaying_radii", "wendland_uniform_radius"])
+@pytest.mark.parametrize("grid", [(128, 128, 16), (128, 128, 144), (256, 256, 160), (128, 128, 160)])
+def test_tensor_form_nyquist_plane(case, grid):
+    """The Nyquist plane l = Kz/2 as two transposed tensor-core jobs (rows b,
+    columns a >= 0; and by conjugate symmetry columns -a > 0 at -Kz/2 with b
+    reversed): 128x128x16 with 128x128 tiles, 128x128x144 (72 planes, not a
+    multiple of 16) with 128x256 tiles, 256x256x160 with CTA pairs.
+    128x128x160 takes CTA pairs for l < 80, whose 256-row m-tiles its 128 b
+    rows cannot fill, so its Nyquist plane stays in the plain form.  The whole
+    plane against FP64 (both signs of a and b, a = -Kx/2 and b = -Ky/2
+    included), and the spectrum against the plain form."""
+    rng = np.random.default_rng(29)
+    groups = _tc_groups(rng, 1001)[case]
+    kx, ky, kz = grid
+    spec_tc, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+    spec_pl, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_PLAIN)
+    a, b = np.meshgrid(np.arange(kx) - kx // 2, np.arange(ky) - ky // 2, indexing="ij")
+    ijk = np.stack([a.ravel(), b.ravel(), np.full(a.size, kz // 2)], 1)
+    ref = sum(O.spectrum_points(g[0], g[1], g[2], 1.0, ijk) for g in groups)
+    assert O.rel_l2(spec_tc[:, :, kz // 2].ravel(), ref) < SPEC_TOL
+    assert O.rel_l2(spec_tc, spec_pl) < SPEC_TOL
+
+
 def test_tensor_form_long_accumulation_random_points():
     """N = 2^18 decaying-Gaussian particles in 16 h-bins on a 64^3 lattice
     (8192 particles ... per item, long TMEM accumulation with flushes);
