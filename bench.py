@@ -48,15 +48,14 @@ def sum_terms_split(w):
     """Terms per step done by the tensor-core kernel if every group takes it,
     and by the plain form.  The planes l < Kz/2 go to the tensor cores, and so
     does the Nyquist plane l = Kz/2 (two transposed jobs in the same launch)
-    when Ky fills whole m-tiles of the tile mode (256 rows for CTA pairs, else
-    128) and Kx/2 whole n-tile units (16 c for CTA pairs, else 8); otherwise
+    when Kx/2 fills whole n-tile units (16 c for CTA pairs, else 8); otherwise
     the plain form sums it.  The rule is the library's tensor_plan."""
     kx, ky, kz = w["grid"]
     n = sum(len(c) for c, _, _ in w["groups"])
     lz_tc = kz // 2
     pairs = os.environ.get("MV_TC_PAIRS", "1")[:1] != "0"
     pair = pairs and lz_tc > 64 and lz_tc % 16 == 0 and (kx * ky) % 256 == 0
-    nyq_tc = ky % (256 if pair else 128) == 0 and (kx // 2) % (16 if pair else 8) == 0 and kx % 2 == 0
+    nyq_tc = ky % 16 == 0 and (kx // 2) % (16 if pair else 8) == 0 and kx % 2 == 0
     plane = n * kx * ky
     return plane * (lz_tc + (1 if nyq_tc else 0)), (0 if nyq_tc else plane)
 

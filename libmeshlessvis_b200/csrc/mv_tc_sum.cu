@@ -631,6 +631,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             // operand scale); the exact 2^-24 is applied with W at the dump
             const double dump_scale = I.job->wmax * (double)kInvProductScale;
             const int rho = I.row0 + row;
+            const bool in_rows = (size_t)rho < mk;  // rows of a partial last m-tile are not dumped
             const int c0 = I.c0;
             const int ncols = 2 * I.nc;
             const int half_cols = 2 * I.bnc;  // columns from one CTA's B rows (all of them unless kPair)
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
 #pragma unroll
                         for (int i = 0; i < 32; ++i) {
                             const int n = cc + i;
-                            if (n < ncols) {
+                            if (n < ncols && in_rows) {
                                 const int h = n / half_cols, nn = n - h * half_cols;
                                 const int im = nn >= I.bnc ? 1 : 0;
                                 const int c = c0 + h * I.bnc + nn - im * I.bnc;
@@ -1113,7 +1114,9 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.nc_tile = ((j.lz_tc + j.n_ntiles - 1) / j.n_ntiles + nc_unit - 1) / nc_unit * nc_unit;
         j.n_ntiles = (j.lz_tc + j.nc_tile - 1) / j.nc_tile;
         const int ctas = mode == kPair ? 2 : 1;
-        j.n_mtiles = (int)((long long)j.kx * j.ky / (kM * ctas));
+        // the last m-tile may extend past the rows (Nyquist jobs): the flush
+        // skips rows >= kx * ky
+        j.n_mtiles = (int)(((long long)j.kx * j.ky + kM * ctas - 1) / (kM * ctas));
         // particle splits: enough items per job for ~tc_waves waves on its
         // own (default 4), at least 64 stages each
         const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
@@ -1193,12 +1196,11 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.wmax = r.weight_max;
         plan.job_of_group.push_back(add_job(j, mode));
         // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
-        // -a > 0; see TcJob) in the same launch, where its Ky rows fill whole
-        // m-tiles of the group's tile mode and its Kx / 2 columns per job split
-        // into whole n-tile units (16 c for kPair, else 8); otherwise the
-        // plain form sums it.
-        const int ctas = mode == kPair ? 2 : 1;
-        if (ky % (kM * ctas) == 0 && (kx / 2) % (mode == kPair ? 16 : 8) == 0 && kx % 2 == 0) {
+        // -a > 0; see TcJob) in the same launch, where the Kx / 2 columns of
+        // each split into whole n-tile units (16 c for kPair, else 8);
+        // otherwise the plain form sums it.  Their Ky rows (8-row chunks of one
+        // sign of b) need not fill the last m-tile.
+        if (ky % 16 == 0 && (kx / 2) % (mode == kPair ? 16 : 8) == 0 && kx % 2 == 0) {
             TcJob t = j;
             t.kx = 1;
             t.ky = ky;

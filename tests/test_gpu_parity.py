@@ -278,16 +278,17 @@ def test_tensor_form_uneven_and_narrowest_n_tiles(case, grid):
 
 
 @pytest.mark.parametrize("case", ["gauss_decaying_radii", "wendland_uniform_radius"])
-@pytest.mark.parametrize("grid", [(128, 128, 16), (128, 128, 144), (256, 256, 160), (128, 128, 160)])
+@pytest.mark.parametrize("grid", [(128, 128, 16), (128, 128, 144), (256, 256, 160), (128, 128, 160),
+                                  (64, 384, 160)])
 def test_tensor_form_nyquist_plane(case, grid):
     """The Nyquist plane l = Kz/2 as two transposed tensor-core jobs (rows b,
     columns a >= 0; and by conjugate symmetry columns -a > 0 at -Kz/2 with b
     reversed): 128x128x16 with 128x128 tiles, 128x128x144 (72 planes, not a
     multiple of 16) with 128x256 tiles, 256x256x160 with CTA pairs.
-    128x128x160 takes CTA pairs for l < 80, whose 256-row m-tiles its 128 b
-    rows cannot fill, so its Nyquist plane stays in the plain form.  The whole
-    plane against FP64 (both signs of a and b, a = -Kx/2 and b = -Ky/2
-    included), and the spectrum against the plain form."""
+    128x128x160 and 64x384x160 take CTA pairs, whose 256-row m-tiles their 128
+    and 384 b rows fill partly: the rows past Ky are computed but not dumped.
+    The whole plane against FP64 (both signs of a and b, a = -Kx/2 and b =
+    -Ky/2 included), and the spectrum against the plain form."""
     rng = np.random.default_rng(29)
     groups = _tc_groups(rng, 1001)[case]
     kx, ky, kz = grid
