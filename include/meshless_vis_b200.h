@@ -116,6 +116,15 @@ int vis_autotune_lookup(int3 grid_size, long long number_of_terms, int number_of
                         int* plain_waves, int* tensor_waves, int* tensor_flush_stages);
 void vis_autotune_clear(void);
 
+/* Device memory the tensor form may use for B-operand images (the c-axis
+ * factors of every particle, computed once per compute and copied by each
+ * m-tile instead of recomputed).  A job whose images would exceed what is left
+ * of the limit computes its B operands per tile instead (same results).
+ * bytes < 0 restores the default: MV_TC_OPERAND_CACHE_MB if set, else a third
+ * of the device's memory; 0 turns the images off.  Process-wide; applies to
+ * later computes.  No counterpart in the reference. */
+void vis_set_operand_cache_limit(long long bytes);
+
 /* ------------------------------------------------------------------ batch */
 /* A batch of jobs, each one registered dataset with its own half-spectrum
  * lattice and its own views and image size (the reference renders one view of

@@ -129,7 +129,7 @@ int tensor_sum_available(const SumRequest& req);
 // One job of the persistent tensor-core kernel: a separable group summed over
 // a lattice of rows (a, b) and columns c >= 0 into an FP64 accumulator.  Its
 // work items are (split ks, m tile, n tile), local index (ks * n_mtiles +
-// m_tile) * n_ntiles + n_tile.  Device-resident (72 bytes).
+// m_tile) * n_ntiles + n_tile.  Device-resident (88 bytes).
 //
 // Frequencies: a = a_idx + a_base, b = b_idx + b_base, c = c_idx + c_base.
 // A group's planes c < Kz/2 are one job (a_base = -Kx/2, b_base = -Ky/2,
@@ -140,6 +140,13 @@ int tensor_sum_available(const SumRequest& req);
 //   a < 0:  F(a, b, Kz/2) = conj F(-a, -b, -Kz/2), so a_base = -Kz/2, rows
 //           b' = -b (b_base = 1 - Ky/2), columns -a = 1 .. Kx/2 (c_base = 1).
 // Every column frequency is >= 0: the B chains only rise.
+//
+// B-operand images: where a job's B stages are read by many m-tiles, they are
+// computed once (tc_bimg_kernel) into `bimg` in the exact swizzled layout of
+// the stage buffer, [n_tile][CTA half][32-particle block][img_stride bytes],
+// each image its hi rows then its lo rows (2 x 2 bnc rows of 128 bytes), and
+// the loader copies them; otherwise (bimg null) producer warps compute them
+// per stage.
 struct TcJob {
     const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
     double* acc;           // [c_idx][Re, Im][a_idx * ky + b_idx]
@@ -153,6 +160,9 @@ struct TcJob {
     int a_base;   // frequency of row index a_idx = 0
     int b_base;   // frequency of row index b_idx = 0 (-Ky/2 or 1 - Ky/2: 8-row chunks never hold both signs)
     int c_base;   // frequency of column c_idx = 0 (>= 0)
+    const unsigned char* bimg;  // B-operand images, or null
+    int n_blocks;    // 32-particle blocks
+    int img_stride;  // bytes per image: 512 x (c values per CTA of a full n-tile)
 };
 
 struct TensorPlan {
@@ -175,6 +185,8 @@ struct TensorPlan {
     std::vector<int> group_class, job_of_group;
     std::vector<int> nyq_job_of_group;  // the transposed Nyquist-plane jobs (a >= 0 here, a < 0 next), or -1
     std::vector<size_t> tp_offset, tp_nyq_offset;
+    std::vector<size_t> bimg_offset;  // per job: its B-operand images in the workspace, or SIZE_MAX
+    size_t bimg_bytes = 0;
     size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
     const void* d_jobs = nullptr;
     const void* d_items = nullptr;
@@ -186,6 +198,7 @@ struct TensorWorkspace {
     Workspace particles;  // per-particle constants of every group
     Workspace acc;        // FP64 accumulators
     Workspace meta;       // job and item tables
+    Workspace bimg;       // B-operand images
     std::vector<char> uploaded;  // the tables last copied to `meta`
     void* uploaded_to = nullptr;
     void release() {
@@ -194,10 +207,16 @@ struct TensorWorkspace {
         particles.release();
         acc.release();
         meta.release();
+        bimg.release();
     }
 };
 
 int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan);
+
+// Device memory the B-operand images of one plan may take: the limit set with
+// vis_set_operand_cache_limit (or MV_TC_OPERAND_CACHE_MB), by default a third
+// of the current device's memory.
+size_t operand_cache_limit();
 int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream);
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag);

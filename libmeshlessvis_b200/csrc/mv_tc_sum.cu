@@ -52,12 +52,17 @@
 //                conflicts), by recurrences along b and
 //                c (8 steps from an exact fixed-point start, moving away from
 //                the axis origin so Gaussian factors only shrink along a chain);
-//   warp 17      streams the per-particle constants of each stage into shared
-//                memory with cp.async.bulk (global -> own CTA, no multicast),
-//                two stages ahead.
+//   warp 17      lane 0 streams the per-particle constants of each stage into
+//                shared memory with cp.async.bulk (global -> own CTA, no
+//                multicast), up to the pipeline depth ahead; lane 1, once the
+//                MMA has read a stage buffer, arrives on its full barrier, for
+//                jobs with B-operand images together with the bulk copy of the
+//                stage's B image (the B warps then idle).
 // Per-particle constants (fixed-point positions, unit rotations, Gaussian
 // ratios) are computed once per launch by tc_prep_kernel into 32-particle
-// field-by-field blocks.
+// field-by-field blocks.  B-operand images (the B stages of a job whose m-tiles
+// all read the same ones) are computed once per launch by tc_bimg_kernel, with
+// the producers' own arithmetic, and read from L2 by every m-tile.
 //
 // Every mbarrier wait is bounded (2 s of %globaltimer); a wait that runs out
 // sets *error_flag, raises the CTA's abort flag, and all roles leave their
@@ -170,6 +175,8 @@ struct TcItem {
     int bc0, bnc;  // the c values whose B rows this CTA produces: all of them, or one half (kPair)
     int row0;      // this CTA's first lattice row
     int a_base, b_base, c_base;  // the job's frequency offsets, in registers for the stage loops
+    const unsigned char* bimg;   // this CTA's B-operand images of the item's n-tile (one per block), or null
+    int img_stride, img_bytes;   // bytes between images; bytes of one image (512 bnc)
 };
 
 template <int MODE>
@@ -194,6 +201,11 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.a_base = r.job->a_base;
     r.b_base = r.job->b_base;
     r.c_base = r.job->c_base;
+    r.img_stride = r.job->img_stride;
+    r.img_bytes = 4 * r.bnc * kRowBytes;
+    r.bimg = r.job->bimg ? r.job->bimg + (size_t)(r.n_tile * Shape<MODE>::kCtas + rank) * r.job->n_blocks *
+                                             (size_t)r.img_stride
+                         : nullptr;
     return r;
 }
 
@@ -478,6 +490,40 @@ __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int 
     }
 }
 
+// One B unit: c values c_s .. c_s + 7 (c_s >= 0; the chain rises) of a
+// particle pair (fixed-point z turns pqz, Gaussian exponents pgam; unit
+// rotations RX, RY, NRY = -RY and Gaussian ratios RHO as in rotate_pair), into
+// a B operand of bnc c values at bhi: rows chunk*8 .. +7 of its Re F half and
+// of its Im F half, hi rows then lo rows 2 bnc rows later.  The producer warps
+// run it into the stage buffer and tc_bimg_kernel into global memory: one
+// arithmetic for both.
+__device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col, int c_s, const uint32_t* pqz,
+                                       const float* pgam, bool gauss, float2 RX, float2 RY, float2 NRY, float2 RHO) {
+    float v[2][3];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        float sn, cs;
+        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
+        float g = kOperandScale, q = 1.f;
+        if (gauss) {
+            g *= exp2f(pgam[e] * (float)(c_s * c_s));
+            q = exp2f(pgam[e] * (float)(2 * c_s + 1));
+        }
+        v[e][0] = g * cs;
+        v[e][1] = -g * sn;
+        v[e][2] = q;
+    }
+    const float2 X = make_float2(v[0][0], v[1][0]);
+    const float2 Y = make_float2(v[0][1], v[1][1]);
+    // bnc and chunk * 8 are multiples of 8: row K of the chain is K within its atom
+    uint8_t* re_base = bhi + chunk * 8 * kRowBytes + (col & 15);
+    uint8_t* im_base = bhi + (bnc + chunk * 8) * kRowBytes + (col & 15);
+    const int c16 = col & ~15;
+    if (gauss) b_chain<true>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY,
+                             make_float2(v[0][2], v[1][2]), RHO);
+    else b_chain<false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, make_float2(1.f, 1.f), RHO);
+}
+
 // Persistent: CTA (or CTA pair) b walks items b, b + grid, ... of the
 // longest-first item list.  Every role walks the same items in the same
 // order, and the pipeline's stage and chain counters (hence mbarrier phases
@@ -523,12 +569,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
 
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) {
-            // one arrival per producer warp, plus (kPair) one from CTA 1's forwarder
-            mbar_init(&full[i], kProducerWarps + (kCtas - 1));
+            // one arrival per producer warp and one from the loader (with the
+            // B image's bytes, if any), plus (kPair) one from CTA 1's forwarder
+            mbar_init(&full[i], kProducerWarps + 1 + (kCtas - 1));
             mbar_init(&empty[i], 1);
             mbar_init(&pdata[i], 1);
             mbar_init(&sfree[i], kProducerWarps);
-            mbar_init(&pfull[i], kProducerWarps);
+            mbar_init(&pfull[i], kProducerWarps + 1);
         }
         for (int i = 0; i < kBufs; ++i) {
             mbar_init(&acc_full[i], 1);
@@ -580,7 +627,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     tc_fence_after();
                     const uint32_t base = smem_u32(smem + buf * kStageBytes);
                     const uint32_t a_hi = base, a_lo = base + kABytes;
-                    const uint32_t b_hi = base + 2 * kABytes, b_lo = b_hi + SH::kBBytes;
+                    // B: hi rows, then lo rows (2 bnc rows each)
+                    const uint32_t b_hi = base + 2 * kABytes, b_lo = b_hi + (uint32_t)(2 * I.bnc * kRowBytes);
                     const uint32_t d = tmem + (uint32_t)(b * SH::kN);
 #pragma unroll
                     for (int t = 0; t < kKr / 16; ++t) {
@@ -718,6 +766,31 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                                   &pdata[buf]);
                 }
             }
+        } else if (lane == 1) {
+            // the loader's arrival on the barrier the MMA waits on (kPair, CTA 1:
+            // the one its forwarder waits on), with the stage's B image where the
+            // job has images.  Both wait until the MMA has read the stage
+            // buffer's previous contents: the copy may then overwrite them, and
+            // the arrival cannot count toward the barrier's previous phase.
+            int S = 0;
+            for (int it = unit; it < a.n_items && !*abort_flag; it += n_units) {
+                const TcItem I = tc_item<MODE>(a, it, rank);
+                int s = 0;
+                for (; s < I.n_stages; ++s, ++S) {
+                    const int buf = S % kStages;
+                    if (!mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 512)) break;
+                    uint64_t* fb = rank == 0 ? &full[buf] : &pfull[buf];
+                    if (I.bimg) {
+                        const int block = I.kb / kBlockParticles + s;
+                        mbar_arrive_expect_tx(fb, (uint32_t)I.img_bytes);
+                        bulk_copy_g2s(smem + buf * kStageBytes + 2 * kABytes, I.bimg + (size_t)block * I.img_stride,
+                                      (uint32_t)I.img_bytes, fb);
+                    } else {
+                        mbar_arrive(fb);
+                    }
+                }
+                if (s < I.n_stages) break;
+            }
         }
         __syncwarp();
     } else {
@@ -837,34 +910,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
 #pragma unroll 1
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
-                        if (chunk * 8 >= I.bnc) break;
-                        const int c_s = I.bc0 + chunk * 8 + I.c_base;  // >= 0: the chain rises
-                        float v[2][3];
-#pragma unroll
-                        for (int e = 0; e < 2; ++e) {
-                            float sn, cs;
-                            __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
-                            float g = kOperandScale, q = 1.f;
-                            if (gauss) {
-                                g *= exp2f(pgam[e] * (float)(c_s * c_s));
-                                q = exp2f(pgam[e] * (float)(2 * c_s + 1));
-                            }
-                            v[e][0] = g * cs;
-                            v[e][1] = -g * sn;
-                            v[e][2] = q;
-                        }
-                        X = make_float2(v[0][0], v[1][0]);
-                        Y = make_float2(v[0][1], v[1][1]);
-                        // nc and chunk * 8 are multiples of 8: row K of the chain is K within its atom
-                        uint8_t* re_base = bhi + chunk * 8 * kRowBytes + (col & 15);
-                        uint8_t* im_base = bhi + (I.bnc + chunk * 8) * kRowBytes + (col & 15);
-                        const int c16 = col & ~15;
-                        if (gauss) {
-                            Q = make_float2(v[0][2], v[1][2]);
-                            b_chain<true>(re_base, im_base, SH::kBBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
-                        } else {
-                            b_chain<false>(re_base, im_base, SH::kBBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
-                        }
+                        if (chunk * 8 >= I.bnc || I.bimg) break;  // the loader copies B images
+                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8 + I.c_base, pqz, pgam, gauss, RX, RY, NRY,
+                               RHO);
                     }
                 }
                 // each thread makes its stores visible to the tensor core; the
@@ -964,6 +1012,42 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
     }
 }
 
+// B-operand images of one job (layout in TcJob): one CTA per image (n-tile,
+// CTA half, 32-particle block); thread (chunk, pair) runs b_unit for 8 c
+// values of 2 particles, exactly as a producer warp would into the stage
+// buffer.  Each image is written once and copied by the tensor kernel's loader
+// for every m-tile of the job.
+struct TcImageArgs {
+    const unsigned char* blocks;
+    unsigned char* bimg;
+    int n_blocks, img_stride;
+    int ctas, nc_tile, lz_tc, c_base;
+    bool gauss;
+};
+
+__global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
+    const long long img = blockIdx.x;  // (n_tile * ctas + half) * n_blocks + block
+    const int block = (int)(img % g.n_blocks);
+    const int nh = (int)(img / g.n_blocks);
+    const int half = nh % g.ctas, n_tile = nh / g.ctas;
+    const int c0 = n_tile * g.nc_tile;
+    const int bnc = min(g.nc_tile, g.lz_tc - c0) / g.ctas;
+    const int pp = threadIdx.x & 15, chunk = threadIdx.x >> 4;
+    if (chunk * 8 >= bnc) return;
+    const unsigned char* blk = g.blocks + (size_t)block * kBlockBytes;
+    const uint2 zq = *reinterpret_cast<const uint2*>(blk + kOffQz + 8 * pp);
+    const uint2 gq = *reinterpret_cast<const uint2*>(blk + kOffGam + 8 * pp);
+    const uint2 rq = *reinterpret_cast<const uint2*>(blk + kOffRho2 + 8 * pp);
+    const float4 r = *reinterpret_cast<const float4*>(blk + kOffRz + 16 * pp);
+    const uint32_t pqz[2] = {zq.x, zq.y};
+    const float pgam[2] = {__uint_as_float(gq.x), __uint_as_float(gq.y)};
+    const float2 RX = make_float2(r.x, r.z), RY = make_float2(r.y, r.w);
+    const float2 NRY = make_float2(-RY.x, -RY.y);
+    const float2 RHO = g.gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
+    uint8_t* out = g.bimg + (size_t)img * g.img_stride;
+    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8 + g.c_base, pqz, pgam, g.gauss, RX, RY, NRY, RHO);
+}
+
 // acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
 // Phi^ factor (groups whose Phi^ factors out) and the scale, written or added.
 // nyquist: the plane c = lz_tc alone, from the transposed jobs' accumulator
@@ -1058,7 +1142,40 @@ int tc_flush_stages(int mode) {
     return mode == kNarrow ? std::min(8, active_tune().tc_flush) : active_tune().tc_flush;
 }
 
+// B-operand images are made for jobs whose every image is copied by at
+// least this many m-tiles.
+constexpr int kImageMinReuse = 4;
+
+long long g_operand_cache_limit = -1;  // bytes; -1: the default policy
+
 }  // namespace
+
+size_t operand_cache_limit() {
+    const long long set = __atomic_load_n(&g_operand_cache_limit, __ATOMIC_RELAXED);
+    if (set >= 0) return (size_t)set;
+    static const long long env = [] {
+        const char* e = std::getenv("MV_TC_OPERAND_CACHE_MB");
+        return e ? std::max(0LL, std::atoll(e)) << 20 : -1LL;
+    }();
+    if (env >= 0) return (size_t)env;
+    // a third of the device's memory, queried once per device
+    static size_t total[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (!total[dev]) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        total[dev] = total_b;
+    }
+    return total[dev] / 3;
+}
+
+extern "C" void vis_set_operand_cache_limit(long long bytes) {
+    __atomic_store_n(&g_operand_cache_limit, bytes < 0 ? -1LL : bytes, __ATOMIC_RELAXED);
+}
 
 int tensor_sum_available(const SumRequest& r) {
     const Lattice& L = r.lat;
@@ -1103,8 +1220,10 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     plan.flush_narrow = tc_flush_stages(kNarrow);
     plan.flush = tc_flush_stages(kWide);
     // Tiles and particle splits of a job (rows kx * ky, columns lz_tc), its
-    // items appended; returns the job's index.
-    auto add_job = [&](TcJob j, int mode) {
+    // items appended, B-operand images where the job allows them (image_ok)
+    // and they fit the limit; returns the job's index.
+    const size_t image_limit = operand_cache_limit();
+    auto add_job = [&](TcJob j, int mode, bool image_ok) {
         // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
         // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
         // shared-memory operand reads); multiples of 16 for kPair
@@ -1126,8 +1245,18 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         const long long chunk = ((j.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
         splits = (j.n + chunk - 1) / chunk;
         j.k_chunk = (int)chunk;
+        j.n_blocks = (j.n + kBlockParticles - 1) / kBlockParticles;
+        j.img_stride = 512 * (j.nc_tile / ctas);
+        j.bimg = nullptr;
+        size_t img_off = SIZE_MAX;
+        const size_t img_total = (size_t)j.n_ntiles * ctas * j.n_blocks * (size_t)j.img_stride;
+        if (image_ok && j.n_mtiles >= kImageMinReuse && plan.bimg_bytes + img_total <= image_limit) {
+            img_off = plan.bimg_bytes;
+            plan.bimg_bytes += img_total;
+        }
         const int job_index = (int)plan.jobs.size();
         plan.jobs.push_back(j);
+        plan.bimg_offset.push_back(img_off);
         const int flush = mode == kNarrow ? plan.flush_narrow : plan.flush;
         for (long long ks = 0; ks < splits; ++ks) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
@@ -1194,7 +1323,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
-        plan.job_of_group.push_back(add_job(j, mode));
+        plan.job_of_group.push_back(add_job(j, mode, true));
         // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
         // -a > 0; see TcJob) in the same launch, where the Kx / 2 columns of
         // each split into whole n-tile units (16 c for kPair, else 8);
@@ -1208,11 +1337,11 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             t.a_base = lz_tc;
             t.b_base = -ky / 2;
             t.c_base = 0;
-            plan.nyq_job_of_group.back() = add_job(t, mode);
+            plan.nyq_job_of_group.back() = add_job(t, mode, false);  // one m-tile: no reuse
             t.a_base = -lz_tc;
             t.b_base = 1 - ky / 2;
             t.c_base = 1;
-            add_job(t, mode);
+            add_job(t, mode, false);
             plan.tp_nyq_offset.back() = plan.tp_bytes;
             plan.tp_bytes += blocks_bytes;
             TensorPlan::Class& c = plan.classes[cls];
@@ -1244,7 +1373,12 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     int st = ws.particles.reserve(std::max<size_t>(plan.tp_bytes, 256));
     if (st == kOk) st = ws.acc.reserve(std::max<size_t>(plan.acc_bytes, 256));
     if (st == kOk) st = ws.meta.reserve(std::max<size_t>(plan.meta_bytes, 256));
+    if (st == kOk && plan.bimg_bytes) st = ws.bimg.reserve(plan.bimg_bytes);
     if (st != kOk) return st;
+    for (size_t j = 0; j < plan.jobs.size(); ++j)
+        plan.jobs[j].bimg = plan.bimg_offset[j] == SIZE_MAX
+                                ? nullptr
+                                : static_cast<const unsigned char*>(ws.bimg.ptr) + plan.bimg_offset[j];
     char* tp_base = static_cast<char*>(ws.particles.ptr);
     char* acc_base = static_cast<char*>(ws.acc.ptr);
     for (size_t g = 0; g < plan.job_of_group.size(); ++g) {
@@ -1311,6 +1445,25 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         count_launch();
     }
     st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
+    if (st != kOk) return st;
+    // B-operand images (after the constants they are made from)
+    for (const TcJob& j : plan.jobs) {
+        if (!j.bimg) continue;
+        TcImageArgs ia;
+        ia.blocks = j.blocks;
+        ia.bimg = const_cast<unsigned char*>(j.bimg);
+        ia.n_blocks = j.n_blocks;
+        ia.img_stride = j.img_stride;
+        ia.ctas = j.img_stride == 512 * j.nc_tile ? 1 : 2;  // 512 nc_tile bytes for one CTA, half for a pair
+        ia.nc_tile = j.nc_tile;
+        ia.lz_tc = j.lz_tc;
+        ia.c_base = j.c_base;
+        ia.gauss = j.gauss != 0;
+        const long long images = (long long)j.n_ntiles * ia.ctas * j.n_blocks;
+        tc_bimg_kernel<<<(unsigned)images, 256, 0, stream>>>(ia);
+        count_launch();
+    }
+    st = check_cuda(cudaGetLastError(), "tc_bimg_kernel launch");
     if (st != kOk) return st;
     // one persistent launch per tile mode for all groups
     if (!plan.items.empty()) {

@@ -301,6 +301,33 @@ def test_tensor_form_nyquist_plane(case, grid):
     assert O.rel_l2(spec_tc, spec_pl) < SPEC_TOL
 
 
+@pytest.mark.parametrize("grid", [(64, 64, 64), (64, 64, 144), (256, 256, 160)])
+def test_tensor_form_operand_images_match_per_tile_operands(grid):
+    """B operands copied from images made once per compute (the default)
+    against B operands computed per tile (vis_set_operand_cache_limit(0)), in
+    128x128 tiles (64^3), 128x256 tiles (72 planes) and CTA pairs
+    (256x256x160); a Gaussian and a factored group.  Both paths run the same
+    arithmetic, and both match FP64."""
+    rng = np.random.default_rng(31)
+    groups = _tc_groups(rng, 2001)["two_groups"]
+    lib = M.lib()
+    try:
+        lib.vis_set_operand_cache_limit(0)
+        spec_tile, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+        lib.vis_set_operand_cache_limit(-1)
+        spec_img, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+    finally:
+        lib.vis_set_operand_cache_limit(-1)
+    assert O.rel_l2(spec_img, spec_tile) < 1e-7
+    kx, ky, kz = grid
+    prng = np.random.default_rng(5)
+    ijk = np.stack([prng.integers(-kx // 2, kx // 2, 2048), prng.integers(-ky // 2, ky // 2, 2048),
+                    prng.integers(0, kz // 2 + 1, 2048)], 1)
+    ref = sum(O.spectrum_points(g[0], g[1], g[2], 1.0, ijk) for g in groups)
+    got = spec_img[ijk[:, 0] + kx // 2, ijk[:, 1] + ky // 2, ijk[:, 2]]
+    assert O.rel_l2(got, ref) < SPEC_TOL
+
+
 def test_tensor_form_long_accumulation_random_points():
     """N = 2^18 decaying-Gaussian particles in 16 h-bins on a 64^3 lattice
     (8192 particles ... per item, long TMEM accumulation with flushes);
