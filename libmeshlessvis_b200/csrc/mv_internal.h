@@ -214,8 +214,8 @@ struct TensorWorkspace {
 int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan);
 
 // Device memory the B-operand images of one plan may take: the limit set with
-// vis_set_operand_cache_limit (or MV_TC_OPERAND_CACHE_MB), by default a third
-// of the current device's memory.
+// vis_set_operand_cache_limit (or MV_TC_OPERAND_CACHE_MB), by default an
+// eighth of the current device's memory.
 size_t operand_cache_limit();
 int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream);
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,

@@ -139,12 +139,23 @@ struct Shape {
     static constexpr int kNc = kN / 2;                       // c values per n-tile (at most)
     static constexpr int kBRows = kN / kCtas;                // B operand rows held by one CTA
     static constexpr int kMTile = kM * kCtas;                // lattice rows per m-tile
-    static constexpr int kStages = MODE == kWide ? 2 : 3;
+    // Rings: A operands (kAStages), B operands (kBStages: deeper where B may
+    // come as a copied image, whose copy starts only once the MMA has read
+    // the B buffer it overwrites), particle constants (kSlots).  One full
+    // barrier per stage, in a ring as deep as the deeper operand ring (an
+    // arrival for stage S + kFull then waits for the MMA to be past stage S).
+    static constexpr int kAStages = 3;
+    static constexpr int kBStages = MODE == kWide ? 2 : 4;
+    static constexpr int kSlots = 2;
+    static constexpr int kFull = kAStages > kBStages ? kAStages : kBStages;
     static constexpr int kBufs = MODE == kNarrow ? 2 : 1;    // TMEM accumulators, kN columns each
     static constexpr int kBBytes = kBRows * kRowBytes;
-    static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
+    static constexpr int kAStageBytes = 2 * kABytes;  // A_hi, A_lo
+    static constexpr int kBStageBytes = 2 * kBBytes;  // B_hi, B_lo (2 bnc rows each, packed)
     static constexpr int kChunksPerThread = kBRows / 128;    // 8-c chunks per B producer thread
-    static constexpr size_t kBarrierOffset = (size_t)kStages * (kStageBytes + kSlotBytes);
+    static constexpr size_t kBOffset = (size_t)kAStages * kAStageBytes;
+    static constexpr size_t kSlotOffset = kBOffset + (size_t)kBStages * kBStageBytes;
+    static constexpr size_t kBarrierOffset = kSlotOffset + (size_t)kSlots * kSlotBytes;
     static constexpr size_t kSmemBytes = kBarrierOffset + 256;
 };
 static_assert(Shape<kNarrow>::kSmemBytes <= 227 * 1024 && Shape<kWide>::kSmemBytes <= 227 * 1024 &&
@@ -531,7 +542,7 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
 // are set up once per CTA.
 //
 // kPair: the barriers that gate the pair's MMAs (full, acc_empty) live in CTA
-// 0 and count the arrivals of both CTAs; the MMA's completion (empty,
+// 0 and count the arrivals of both CTAs; the MMA's completion (a_empty, b_empty,
 // acc_full, drain) is signalled to both CTAs by multicast commits; each CTA's
 // loader, producers and flush warps otherwise work on their own shared memory
 // and TMEM.  Cluster barriers after set-up and before exit keep each CTA's
@@ -539,16 +550,20 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     using SH = Shape<MODE>;
-    constexpr int kStages = SH::kStages, kStageBytes = SH::kStageBytes, kBufs = SH::kBufs, kCtas = SH::kCtas;
+    constexpr int kAStages = SH::kAStages, kBStages = SH::kBStages, kSlots = SH::kSlots, kFull = SH::kFull;
+    constexpr int kBufs = SH::kBufs, kCtas = SH::kCtas;
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* slots = smem + kStages * kStageBytes;  // [kStages][kSlotBytes]
+    uint8_t* a_ring = smem;                   // [kAStages][kAStageBytes]
+    uint8_t* b_ring = smem + SH::kBOffset;    // [kBStages][kBStageBytes]
+    uint8_t* slots = smem + SH::kSlotOffset;  // [kSlots][kSlotBytes]
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SH::kBarrierOffset);
-    uint64_t* full = bars;                   // [kStages] producers -> MMA (CTA 0's)
-    uint64_t* empty = bars + kStages;        // [kStages] MMA -> producers
-    uint64_t* pdata = bars + 2 * kStages;    // [kStages] loader -> producers
-    uint64_t* sfree = bars + 3 * kStages;    // [kStages] producers -> loader: the slot has been read
-    uint64_t* pfull = bars + 4 * kStages;    // [kStages] kPair, CTA 1: its producers -> its forwarder
-    uint64_t* acc_full = bars + 5 * kStages;   // [kBufs] MMA -> flush: a chain is complete
+    uint64_t* full = bars;                        // [kFull] producers, loader -> MMA (CTA 0's)
+    uint64_t* pfull = full + kFull;               // [kFull] kPair, CTA 1: its producers, loader -> its forwarder
+    uint64_t* a_empty = pfull + kFull;            // [kAStages] MMA -> A producers
+    uint64_t* b_empty = a_empty + kAStages;       // [kBStages] MMA -> B producers, loader
+    uint64_t* pdata = b_empty + kBStages;         // [kSlots] loader -> producers
+    uint64_t* sfree = pdata + kSlots;             // [kSlots] producers -> loader: the slot has been read
+    uint64_t* acc_full = sfree + kSlots;          // [kBufs] MMA -> flush: a chain is complete
     uint64_t* acc_empty = acc_full + 2;         // [kBufs] flush -> MMA (CTA 0's): the accumulator has been read
     uint64_t* drain = acc_full + 4;
     volatile uint32_t* tmem_slot = reinterpret_cast<volatile uint32_t*>(acc_full + 5);
@@ -568,14 +583,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     }
 
     if (tid == 0) {
-        for (int i = 0; i < kStages; ++i) {
+        for (int i = 0; i < kFull; ++i) {
             // one arrival per producer warp and one from the loader (with the
             // B image's bytes, if any), plus (kPair) one from CTA 1's forwarder
             mbar_init(&full[i], kProducerWarps + 1 + (kCtas - 1));
-            mbar_init(&empty[i], 1);
+            mbar_init(&pfull[i], kProducerWarps + 1);
+        }
+        for (int i = 0; i < kAStages; ++i) mbar_init(&a_empty[i], 1);
+        for (int i = 0; i < kBStages; ++i) mbar_init(&b_empty[i], 1);
+        for (int i = 0; i < kSlots; ++i) {
             mbar_init(&pdata[i], 1);
             mbar_init(&sfree[i], kProducerWarps);
-            mbar_init(&pfull[i], kProducerWarps + 1);
         }
         for (int i = 0; i < kBufs; ++i) {
             mbar_init(&acc_full[i], 1);
@@ -617,18 +635,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 const TcItem I = tc_item<MODE>(a, it, 0);
                 const uint32_t idesc = mma_idesc(kM * kCtas, 2 * I.nc);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
-                    const int buf = S % kStages;
+                    const int fb = S % kFull, ab = S % kAStages, bb = S % kBStages;
                     const int k = C + s / flush_stages;  // chain index
                     const int b = k % kBufs, u = k / kBufs;  // accumulator and its use count
                     const bool first = (s % flush_stages) == 0;
                     // a chain starts once the flush of the accumulator's previous chain has read it
                     if (first && u >= 1 && !mbar_wait(&acc_empty[b], (u - 1) & 1, abort_flag, a.error_flag, 1)) break;
-                    if (!mbar_wait(&full[buf], (S / kStages) & 1, abort_flag, a.error_flag, 2)) break;
+                    if (!mbar_wait(&full[fb], (S / kFull) & 1, abort_flag, a.error_flag, 2)) break;
                     tc_fence_after();
-                    const uint32_t base = smem_u32(smem + buf * kStageBytes);
-                    const uint32_t a_hi = base, a_lo = base + kABytes;
+                    const uint32_t a_hi = smem_u32(a_ring + ab * SH::kAStageBytes), a_lo = a_hi + kABytes;
                     // B: hi rows, then lo rows (2 bnc rows each)
-                    const uint32_t b_hi = base + 2 * kABytes, b_lo = b_hi + (uint32_t)(2 * I.bnc * kRowBytes);
+                    const uint32_t b_hi = smem_u32(b_ring + bb * SH::kBStageBytes);
+                    const uint32_t b_lo = b_hi + (uint32_t)(2 * I.bnc * kRowBytes);
                     const uint32_t d = tmem + (uint32_t)(b * SH::kN);
 #pragma unroll
                     for (int t = 0; t < kKr / 16; ++t) {
@@ -638,7 +656,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         mma_f16<kCtas>(d, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
                         mma_f16<kCtas>(d, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, 1u);
                     }
-                    mma_commit<kCtas>(&empty[buf]);
+                    mma_commit<kCtas>(&a_empty[ab]);
+                    mma_commit<kCtas>(&b_empty[bb]);
                     if ((s % flush_stages) == flush_stages - 1 || s == I.n_stages - 1) mma_commit<kCtas>(&acc_full[b]);
                 }
                 C += I.n_chunks;
@@ -656,9 +675,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     const TcItem I = tc_item<MODE>(a, it, 1);
                     int s = 0;
                     for (; s < I.n_stages; ++s, ++S) {
-                        const int buf = S % kStages;
-                        if (!mbar_wait(&pfull[buf], (S / kStages) & 1, abort_flag, a.error_flag, 256)) break;
-                        mbar_arrive_leader(&full[buf]);
+                        const int fb = S % kFull;
+                        if (!mbar_wait(&pfull[fb], (S / kFull) & 1, abort_flag, a.error_flag, 256)) break;
+                        mbar_arrive_leader(&full[fb]);
                     }
                     if (s < I.n_stages) break;
                 }
@@ -755,10 +774,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             for (int it = unit; it < a.n_items && !*abort_flag; it += n_units) {
                 const TcItem I = tc_item<MODE>(a, it, rank);
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
-                    const int buf = S % kStages;
-                    // this CTA's producers have read the slot's constants of stage S - kStages
-                    if (S >= kStages &&
-                        !mbar_wait(&sfree[buf], ((S / kStages) - 1) & 1, abort_flag, a.error_flag, 32))
+                    const int buf = S % kSlots;
+                    // this CTA's producers have read the slot's constants of stage S - kSlots
+                    if (S >= kSlots && !mbar_wait(&sfree[buf], ((S / kSlots) - 1) & 1, abort_flag, a.error_flag, 32))
                         break;
                     const int block = I.kb / kBlockParticles + s;
                     mbar_arrive_expect_tx(&pdata[buf], kBlockBytes);
@@ -777,13 +795,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 const TcItem I = tc_item<MODE>(a, it, rank);
                 int s = 0;
                 for (; s < I.n_stages; ++s, ++S) {
-                    const int buf = S % kStages;
-                    if (!mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 512)) break;
-                    uint64_t* fb = rank == 0 ? &full[buf] : &pfull[buf];
+                    const int bb = S % kBStages;
+                    if (!mbar_wait(&b_empty[bb], ((S / kBStages) & 1) ^ 1, abort_flag, a.error_flag, 512)) break;
+                    uint64_t* fb = rank == 0 ? &full[S % kFull] : &pfull[S % kFull];
                     if (I.bimg) {
                         const int block = I.kb / kBlockParticles + s;
                         mbar_arrive_expect_tx(fb, (uint32_t)I.img_bytes);
-                        bulk_copy_g2s(smem + buf * kStageBytes + 2 * kABytes, I.bimg + (size_t)block * I.img_stride,
+                        bulk_copy_g2s(b_ring + bb * SH::kBStageBytes, I.bimg + (size_t)block * I.img_stride,
                                       (uint32_t)I.img_bytes, fb);
                     } else {
                         mbar_arrive(fb);
@@ -811,8 +829,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             const bool a_up = b0 >= 0;
             const int b_s = a_up ? b0 : b0 + 7;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
-                const int buf = S % kStages;
-                if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kStages) & 1, abort_flag, a.error_flag, 64)))
+                const int buf = S % kSlots;
+                if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kSlots) & 1, abort_flag, a.error_flag, 64)))
                     break;
                 uint32_t pqx[2], pqy[2], pqz[2];
                 float pamp[2], pgam[2], prho2[2];
@@ -856,10 +874,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 // the slot's constants are in registers: release it to the loader
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&sfree[buf]);
-                if (!__all_sync(0xffffffffu,
-                                mbar_wait(&empty[buf], ((S / kStages) & 1) ^ 1, abort_flag, a.error_flag, 8)))
-                    break;
-                uint8_t* st = smem + buf * kStageBytes;
+                // the ring buffer this warp writes: A or B
+                const bool waited = has_a ? mbar_wait(&a_empty[S % kAStages], ((S / kAStages) & 1) ^ 1, abort_flag,
+                                                      a.error_flag, 8)
+                                          : mbar_wait(&b_empty[S % kBStages], ((S / kBStages) & 1) ^ 1, abort_flag,
+                                                      a.error_flag, 8);
+                if (!__all_sync(0xffffffffu, waited)) break;
+                uint8_t* st = has_a ? a_ring + (S % kAStages) * SH::kAStageBytes
+                                    : b_ring + (S % kBStages) * SH::kBStageBytes;
                 // the thread's two particles as packed pairs (see split_pair)
                 float2 X, Y, RX, RY, Q = make_float2(1.f, 1.f), RHO = make_float2(1.f, 1.f);
                 const int col = 8 * pp;  // byte offset of the pair within a 128-byte operand row
@@ -902,7 +924,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     // from bc0 (8 each), scaled by 2^12; rows [0, bnc) hold (Re B, -Im B)
                     // pairs (Re F columns), rows [bnc, 2 bnc) (Im B, Re B) (Im F columns).
                     // Chunks at or beyond bnc are not read by the MMA.
-                    uint8_t* bhi = st + 2 * kABytes;
+                    uint8_t* bhi = st;
                     RX = make_float2(prz[0].x, prz[1].x);
                     RY = make_float2(prz[0].y, prz[1].y);
                     const float2 NRY = make_float2(-RY.x, -RY.y);
@@ -921,8 +943,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 __syncwarp();
                 if (lane == 0) {
                     // kPair: CTA 1's warps report to their forwarder (see the MMA role)
-                    if (rank == 0) mbar_arrive(&full[buf]);
-                    else mbar_arrive(&pfull[buf]);
+                    if (rank == 0) mbar_arrive(&full[S % kFull]);
+                    else mbar_arrive(&pfull[S % kFull]);
                 }
             }
         }
@@ -1158,7 +1180,7 @@ size_t operand_cache_limit() {
         return e ? std::max(0LL, std::atoll(e)) << 20 : -1LL;
     }();
     if (env >= 0) return (size_t)env;
-    // a third of the device's memory, queried once per device
+    // an eighth of the device's memory, queried once per device
     static size_t total[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
@@ -1170,7 +1192,7 @@ size_t operand_cache_limit() {
         }
         total[dev] = total_b;
     }
-    return total[dev] / 3;
+    return total[dev] / 8;
 }
 
 extern "C" void vis_set_operand_cache_limit(long long bytes) {
