@@ -239,11 +239,16 @@ __global__ void __launch_bounds__(kThreads, 2) plain_sum_kernel(SumKernelArgs a)
 // packed FP32 FMA (sm_100 FFMA2) each.
 // Terms outside the lattice and the mirrors of xp = 0 / yp = 0 are computed
 // but not stored.  The partial-sum layout is the plain kernel's.
+// Each 256-particle tile is summed in FP32 registers and added to the
+// thread's running sums in FP64, which live in global scratch (read and
+// written once per tile, coalesced across the warp), so L is bounded by the
+// tile accumulators alone.
 struct FoldKernelArgs {
     SumKernelArgs s;
     int xpc;       // x chunks of L representatives: ceil(XP / L)
     int yrows;     // FY == 2: YP representatives yp; FY == 1: lat.ny
     size_t plane;  // partial sums per split: lat.nx * n_rest
+    double2* sums;  // [split][L * 2 FY][gridDim.x * kThreads] running FP64 sums
 };
 
 template <int L, int FY, int AMP>
@@ -282,11 +287,8 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
     }
 
     constexpr int NP = 2 * FY;  // packed pairs of real sums per representative
-    float2 tot[L][NP], comp[L][NP];
-#pragma unroll
-    for (int m = 0; m < L; ++m)
-#pragma unroll
-        for (int i = 0; i < NP; ++i) tot[m][i] = comp[m][i] = make_float2(0.f, 0.f);
+    const size_t tstride = (size_t)gridDim.x * kThreads;
+    double2* sums = fa.sums + (size_t)blockIdx.y * (L * NP) * tstride + t;  // this thread's, stride tstride
 
     const int beg = blockIdx.y * a.chunk;
     const int end = min(a.n, beg + a.chunk);
@@ -374,20 +376,20 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
                 }
             }
         }
-        // Kahan: add this tile's sums to the running totals.
+        // add this tile's sums to the running FP64 sums
+        const bool first = t0 == beg;
 #pragma unroll
         for (int m = 0; m < L; ++m)
 #pragma unroll
             for (int i = 0; i < NP; ++i) {
-                const float2 yv = __fadd2_rn(acc[m][i], make_float2(-comp[m][i].x, -comp[m][i].y));
-                const float2 tv = __fadd2_rn(tot[m][i], yv);
-                const float2 dt = __fadd2_rn(tv, make_float2(-tot[m][i].x, -tot[m][i].y));
-                comp[m][i] = __fadd2_rn(dt, make_float2(-yv.x, -yv.y));
-                tot[m][i] = tv;
+                double2* p = sums + (size_t)(m * NP + i) * tstride;
+                const double2 o = first ? make_double2(0.0, 0.0) : *p;
+                *p = make_double2(o.x + (double)acc[m][i].x, o.y + (double)acc[m][i].y);
             }
     }
 
     if (!active) return;
+    const bool any = beg < end;
     float2* out = a.partial + blockIdx.y * fa.plane;
     const int x_lo = a.lat.x0, x_hi = a.lat.x0 + a.lat.nx - 1;
     const int y_lo = a.lat.y0, y_hi = a.lat.y0 + a.lat.ny - 1;
@@ -400,13 +402,14 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
             if (sy == 1 && yp == 0) continue;
             if (y < y_lo || y > y_hi) continue;
             // (A0, A3) and (A2, A1) of this y sign
-            const float2 p0 = make_float2(tot[m][2 * sy].x - comp[m][2 * sy].x, tot[m][2 * sy].y - comp[m][2 * sy].y);
-            const float2 p1 =
-                make_float2(tot[m][2 * sy + 1].x - comp[m][2 * sy + 1].x, tot[m][2 * sy + 1].y - comp[m][2 * sy + 1].y);
+            const double2 z2 = make_double2(0.0, 0.0);
+            const double2 p0 = any ? sums[(size_t)(m * NP + 2 * sy) * tstride] : z2;
+            const double2 p1 = any ? sums[(size_t)(m * NP + 2 * sy + 1) * tstride] : z2;
             const size_t rest = (size_t)(y - y_lo) * nz + (z - a.lat.z0);
-            if (xp <= x_hi) out[(size_t)(xp - x_lo) * a.n_rest + rest] = make_float2(p0.x - p1.y, p1.x + p0.y);
+            if (xp <= x_hi)
+                out[(size_t)(xp - x_lo) * a.n_rest + rest] = make_float2((float)(p0.x - p1.y), (float)(p1.x + p0.y));
             if (xp > 0 && -xp >= x_lo)
-                out[(size_t)(-xp - x_lo) * a.n_rest + rest] = make_float2(p0.x + p1.y, p1.x - p0.y);
+                out[(size_t)(-xp - x_lo) * a.n_rest + rest] = make_float2((float)(p0.x + p1.y), (float)(p1.x - p0.y));
         }
     }
 }
@@ -549,11 +552,26 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     const int nxc = (lat.nx + L - 1) / L;
     const long long n_rest = (long long)lat.ny * lat.nz;
     // Folded form when x = 0 is on the lattice (and y folds too when the y
-    // range holds both signs): L = 4 x representatives with y folded, else 8.
+    // range holds both signs).  x representatives per thread: 8 without the y
+    // fold; with it the L of {4, 5, 6} (more spill at 128 registers) that
+    // minimises the chunks' work, ceil(XP / L) (30 + 20 L) instructions per
+    // particle (a particle's phases and constants, then one Phi^ evaluation
+    // and x rotation per representative): 65 representatives (C2's 128^3) and
+    // 33 (64^3) take 6.
     const bool fold = lat.x0 <= 0 && lat.x0 + lat.nx - 1 >= 0;
     const bool fold_y = fold && lat.y0 < 0 && lat.y0 + lat.ny - 1 > 0;
-    const int fold_l = fold_y ? 4 : 8;
     const int xp_count = std::max(-lat.x0, lat.x0 + lat.nx - 1) + 1;
+    int fold_l = 8;
+    if (fold_y) {
+        long long best = -1;
+        for (int l : {4, 5, 6}) {
+            const long long cost = (long long)((xp_count + l - 1) / l) * (30 + 20 * l);
+            if (best < 0 || cost < best) {
+                best = cost;
+                fold_l = l;
+            }
+        }
+    }
     const int yrows = fold_y ? std::max(-lat.y0, lat.y0 + lat.ny - 1) + 1 : lat.ny;
     const int xpc = (xp_count + fold_l - 1) / fold_l;
     const long long threads = fold ? (long long)xpc * yrows * lat.nz : (long long)nxc * n_rest;
@@ -589,7 +607,11 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     const size_t plane = fold ? (size_t)lat.nx * n_rest : (size_t)nxc * L * n_rest;
     const size_t part_bytes = (plane * splits * sizeof(float2) + 255) / 256 * 256;
     const size_t table_cells = amp == kAmpTable ? (size_t)table_n + 1 : 0;
-    int st = ws.reserve(part_bytes + table_cells * sizeof(float4));
+    const size_t table_bytes = (table_cells * sizeof(float4) + 255) / 256 * 256;
+    // folded form: the running FP64 sums, 2 FY pairs per representative
+    const size_t sums_bytes =
+        fold ? (size_t)splits * fold_l * (fold_y ? 4 : 2) * (size_t)blocks_f * kThreads * sizeof(double2) : 0;
+    int st = ws.reserve(part_bytes + table_bytes + sums_bytes);
     if (st != kOk) return st;
 
     SumKernelArgs a;
@@ -619,7 +641,11 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         fa.xpc = xpc;
         fa.yrows = yrows;
         fa.plane = plane;
-        FoldKernel k = fold_y ? pick_fold<4, 2>(amp) : pick_fold<8, 1>(amp);
+        fa.sums = reinterpret_cast<double2*>(static_cast<char*>(ws.ptr) + part_bytes + table_bytes);
+        FoldKernel k = !fold_y        ? pick_fold<8, 1>(amp)
+                       : fold_l == 4 ? pick_fold<4, 2>(amp)
+                       : fold_l == 5 ? pick_fold<5, 2>(amp)
+                                     : pick_fold<6, 2>(amp);
         if (dyn_smem > 48 * 1024) {
             st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
                             "cudaFuncSetAttribute");
