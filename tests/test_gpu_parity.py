@@ -328,6 +328,33 @@ def test_tensor_form_operand_images_match_per_tile_operands(grid):
     assert O.rel_l2(got, ref) < SPEC_TOL
 
 
+def test_tensor_form_operand_cache_limit_covers_some_jobs():
+    """A limit that holds the first group's B-operand images but not the
+    second's: one launch mixes image jobs and per-tile jobs (and the Nyquist
+    jobs, which never use images).  Same spectrum as with the images off."""
+    rng = np.random.default_rng(37)
+    n = 1000
+    groups = []
+    for k in range(2):
+        pos = rng.random((n, 3), dtype=np.float32)
+        w = rng.standard_normal(n).astype(np.float32)
+        h = np.exp(rng.uniform(np.log(0.01), np.log(0.05), n)).astype(np.float32)
+        groups.append((constraints(pos, w), h, M.GAUSSIAN_DECAYING))
+    grid = (64, 64, 64)
+    # images of one group: 32 blocks x 1 n-tile x 32 c values x 512 B = 512 KiB
+    lib = M.lib()
+    try:
+        lib.vis_set_operand_cache_limit(0)
+        spec_tile, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+        lib.vis_set_operand_cache_limit(600 * 1024)
+        spec_mix, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (16, 16), (32, 32), None, M.FORM_TENSOR)
+    finally:
+        lib.vis_set_operand_cache_limit(-1)
+    assert O.rel_l2(spec_mix, spec_tile) < 1e-7
+    ref = O.spectrum_grid(groups, 1.0, grid)
+    assert O.rel_l2(spec_mix, ref) < SPEC_TOL
+
+
 def test_tensor_form_long_accumulation_random_points():
     """N = 2^18 decaying-Gaussian particles in 16 h-bins on a 64^3 lattice
     (8192 particles ... per item, long TMEM accumulation with flushes);
