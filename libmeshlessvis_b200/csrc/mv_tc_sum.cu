@@ -130,12 +130,20 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 //       stage for twice its work, and the MMA reads 64 B/clk of shared memory
 //       per CTA.  Used where the tensor planes are a multiple of 16 and the
 //       rows a multiple of 256.
-enum TileMode : int { kNarrow = 0, kWide = 1, kPair = 2 };
+//   kPairNarrow: the CTA pair for lattices with at most 64 tensor planes
+//       (planes a multiple of 16, rows of 256): one 256x128 MMA, two
+//       alternating 128-column accumulators per CTA as in kNarrow.  Each CTA
+//       reads A and half of B, 96 B/clk at the tensor core's rate, where a
+//       128x128 MMA needs the port's full 128 B/clk; B work per CTA halves.
+enum TileMode : int { kNarrow = 0, kWide = 1, kPair = 2, kPairNarrow = 3 };
+
+constexpr bool pair_mode(int mode) { return mode == kPair || mode == kPairNarrow; }
+constexpr bool narrow_mode(int mode) { return mode == kNarrow || mode == kPairNarrow; }
 
 template <int MODE>
 struct Shape {
-    static constexpr int kCtas = MODE == kPair ? 2 : 1;
-    static constexpr int kN = MODE == kNarrow ? 128 : 256;  // accumulator columns: the MMA's N at most
+    static constexpr int kCtas = pair_mode(MODE) ? 2 : 1;
+    static constexpr int kN = narrow_mode(MODE) ? 128 : 256;  // accumulator columns: the MMA's N at most
     static constexpr int kNc = kN / 2;                       // c values per n-tile (at most)
     static constexpr int kBRows = kN / kCtas;                // B operand rows held by one CTA
     static constexpr int kMTile = kM * kCtas;                // lattice rows per m-tile
@@ -148,18 +156,18 @@ struct Shape {
     static constexpr int kBStages = MODE == kWide ? 2 : 4;
     static constexpr int kSlots = 2;
     static constexpr int kFull = kAStages > kBStages ? kAStages : kBStages;
-    static constexpr int kBufs = MODE == kNarrow ? 2 : 1;    // TMEM accumulators, kN columns each
+    static constexpr int kBufs = narrow_mode(MODE) ? 2 : 1;  // TMEM accumulators, kN columns each
     static constexpr int kBBytes = kBRows * kRowBytes;
     static constexpr int kAStageBytes = 2 * kABytes;  // A_hi, A_lo
     static constexpr int kBStageBytes = 2 * kBBytes;  // B_hi, B_lo (2 bnc rows each, packed)
-    static constexpr int kChunksPerThread = kBRows / 128;    // 8-c chunks per B producer thread
+    static constexpr int kChunksPerThread = kBRows > 128 ? kBRows / 128 : 1;  // 8-c chunks per B producer thread
     static constexpr size_t kBOffset = (size_t)kAStages * kAStageBytes;
     static constexpr size_t kSlotOffset = kBOffset + (size_t)kBStages * kBStageBytes;
     static constexpr size_t kBarrierOffset = kSlotOffset + (size_t)kSlots * kSlotBytes;
     static constexpr size_t kSmemBytes = kBarrierOffset + 256;
 };
 static_assert(Shape<kNarrow>::kSmemBytes <= 227 * 1024 && Shape<kWide>::kSmemBytes <= 227 * 1024 &&
-                  Shape<kPair>::kSmemBytes <= 227 * 1024,
+                  Shape<kPair>::kSmemBytes <= 227 * 1024 && Shape<kPairNarrow>::kSmemBytes <= 227 * 1024,
               "shared memory");
 
 // idesc of tcgen05.mma kind::f16: D F32, A/B F16, both K-major, M = m, N = n.
@@ -1161,7 +1169,7 @@ int tc_flush_stages(int mode) {
         return (x >= 1 && x <= 1024) ? x : 0;
     }();
     if (env) return env;
-    return mode == kNarrow ? std::min(8, active_tune().tc_flush) : active_tune().tc_flush;
+    return narrow_mode(mode) ? std::min(8, active_tune().tc_flush) : active_tune().tc_flush;
 }
 
 // B-operand images are made for jobs whose every image is copied by at
@@ -1249,12 +1257,12 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
         // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
         // shared-memory operand reads); multiples of 16 for kPair
-        const int nc_max = mode == kNarrow ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
-        const int nc_unit = mode == kPair ? 16 : 8;
+        const int nc_max = narrow_mode(mode) ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
+        const int nc_unit = pair_mode(mode) ? 16 : 8;
         j.n_ntiles = (j.lz_tc + nc_max - 1) / nc_max;
         j.nc_tile = ((j.lz_tc + j.n_ntiles - 1) / j.n_ntiles + nc_unit - 1) / nc_unit * nc_unit;
         j.n_ntiles = (j.lz_tc + j.nc_tile - 1) / j.nc_tile;
-        const int ctas = mode == kPair ? 2 : 1;
+        const int ctas = pair_mode(mode) ? 2 : 1;
         // the last m-tile may extend past the rows (Nyquist jobs): the flush
         // skips rows >= kx * ky
         j.n_mtiles = (int)(((long long)j.kx * j.ky + kM * ctas - 1) / (kM * ctas));
@@ -1279,7 +1287,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         const int job_index = (int)plan.jobs.size();
         plan.jobs.push_back(j);
         plan.bimg_offset.push_back(img_off);
-        const int flush = mode == kNarrow ? plan.flush_narrow : plan.flush;
+        const int flush = narrow_mode(mode) ? plan.flush_narrow : plan.flush;
         for (long long ks = 0; ks < splits; ++ks) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
             const long long stages = (k1 - k0 + kKp - 1) / kKp;
@@ -1332,9 +1340,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         // tile mode: kNarrow up to 64 tensor planes; beyond, kPair where every
         // n-tile splits into two halves of 8-c chunks and the rows into
         // 256-row m-tiles, else kWide
-        const int mode = lz_tc <= Shape<kNarrow>::kNc                                         ? kNarrow
-                         : (tc_pairs_enabled() && lz_tc % 16 == 0 && ((long long)kx * ky) % 256 == 0) ? kPair
-                                                                                                    : kWide;
+        const bool pairs = tc_pairs_enabled() && lz_tc % 16 == 0 && ((long long)kx * ky) % 256 == 0;
+        const int mode = lz_tc <= Shape<kNarrow>::kNc ? (pairs ? kPairNarrow : kNarrow) : (pairs ? kPair : kWide);
         TcJob j{};
         j.kx = kx;
         j.ky = ky;
@@ -1351,7 +1358,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         // each split into whole n-tile units (16 c for kPair, else 8);
         // otherwise the plain form sums it.  Their Ky rows (8-row chunks of one
         // sign of b) need not fill the last m-tile.
-        if (ky % 16 == 0 && (kx / 2) % (mode == kPair ? 16 : 8) == 0 && kx % 2 == 0) {
+        if (ky % 16 == 0 && (kx / 2) % (pair_mode(mode) ? 16 : 8) == 0 && kx % 2 == 0) {
             TcJob t = j;
             t.kx = 1;
             t.ky = ky;
@@ -1376,15 +1383,16 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
     // per tile mode, longest first (round-robin over the persistent CTAs / pairs)
-    auto order = [](int m) { return m == kNarrow ? 0 : m == kPair ? 1 : 2; };
+    auto order = [](int m) { return m == kNarrow ? 0 : m == kPairNarrow ? 1 : m == kPair ? 2 : 3; };
     std::stable_sort(items.begin(), items.end(), [&](const Item& x, const Item& y) {
         return x.mode != y.mode ? order(x.mode) < order(y.mode) : x.cost > y.cost;
     });
     plan.items.reserve(items.size());
-    plan.n_narrow = plan.n_pair = 0;
+    plan.n_narrow = plan.n_pair_narrow = plan.n_pair = 0;
     for (auto& it : items) {
         plan.items.push_back(it.item);
         plan.n_narrow += it.mode == kNarrow ? 1 : 0;
+        plan.n_pair_narrow += it.mode == kPairNarrow ? 1 : 0;
         plan.n_pair += it.mode == kPair ? 1 : 0;
     }
     plan.meta_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256 + plan.items.size() * sizeof(int2);
@@ -1439,6 +1447,46 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     return kOk;
 }
 
+namespace {
+
+// One persistent launch of a tile mode: min(items, SMs) CTAs, or for the CTA
+// pair modes clusters of 2, as many as can be resident at once.
+template <int MODE>
+int launch_tile(const TcArgs& a, cudaStream_t stream) {
+    using SH = Shape<MODE>;
+    int st = check_cuda(
+        cudaFuncSetAttribute(tc_sum_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::kSmemBytes),
+        "cudaFuncSetAttribute");
+    if (st != kOk) return st;
+    if constexpr (SH::kCtas == 1) {
+        const int grid = std::min<int>(a.n_items, device_sm_count());
+        tc_sum_kernel<MODE><<<grid, kThreads, SH::kSmemBytes, stream>>>(a);
+        return kOk;
+    } else {
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.blockDim = dim3(kThreads);
+        lc.dynamicSmemBytes = SH::kSmemBytes;
+        lc.stream = stream;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        lc.gridDim = dim3(2 * std::max(1, device_sm_count() / 2));
+        int clusters = 0;
+        st = check_cuda(cudaOccupancyMaxActiveClusters(&clusters, tc_sum_kernel<MODE>, &lc),
+                        "cudaOccupancyMaxActiveClusters");
+        if (st != kOk) return st;
+        if (clusters < 1) return set_error(kCudaError, "tensor sum: no CTA pair fits on this device");
+        lc.gridDim = dim3(2 * std::min(a.n_items, clusters));
+        return check_cuda(cudaLaunchKernelEx(&lc, tc_sum_kernel<MODE>, a), "tc_sum_kernel (pairs) launch");
+    }
+}
+
+}  // namespace
+
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag) {
     int st = kOk;
@@ -1490,60 +1538,25 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
     // one persistent launch per tile mode for all groups
     if (!plan.items.empty()) {
         timer_begin(timer, 3, stream);
-        const int counts[3] = {plan.n_narrow, plan.n_pair, (int)plan.items.size() - plan.n_narrow - plan.n_pair};
+        const int counts[4] = {plan.n_narrow, plan.n_pair_narrow, plan.n_pair,
+                               (int)plan.items.size() - plan.n_narrow - plan.n_pair_narrow - plan.n_pair};
+        const int modes[4] = {kNarrow, kPairNarrow, kPair, kWide};
         int first = 0;
-        for (int m = 0; m < 3 && st == kOk; first += counts[m], ++m) {
+        for (int m = 0; m < 4 && st == kOk; first += counts[m], ++m) {
             TcArgs a;
             a.jobs = static_cast<const TcJob*>(plan.d_jobs);
             a.items = static_cast<const int2*>(plan.d_items) + first;
             a.n_items = counts[m];
-            a.flush_stages = m == 0 ? plan.flush_narrow : plan.flush;
+            a.flush_stages = narrow_mode(modes[m]) ? plan.flush_narrow : plan.flush;
             a.error_flag = error_flag;
             if (a.n_items == 0) continue;
-            if (m == 0) {
-                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kNarrow>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)Shape<kNarrow>::kSmemBytes),
-                                "cudaFuncSetAttribute");
-                if (st != kOk) break;
-                const int grid = std::min<int>(a.n_items, device_sm_count());
-                tc_sum_kernel<kNarrow><<<grid, kThreads, Shape<kNarrow>::kSmemBytes, stream>>>(a);
-            } else if (m == 2) {
-                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kWide>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)Shape<kWide>::kSmemBytes),
-                                "cudaFuncSetAttribute");
-                if (st != kOk) break;
-                const int grid = std::min<int>(a.n_items, device_sm_count());
-                tc_sum_kernel<kWide><<<grid, kThreads, Shape<kWide>::kSmemBytes, stream>>>(a);
-            } else {
-                // CTA pairs: clusters of 2, as many as can be resident at once
-                st = check_cuda(cudaFuncSetAttribute(tc_sum_kernel<kPair>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     (int)Shape<kPair>::kSmemBytes),
-                                "cudaFuncSetAttribute");
-                if (st != kOk) break;
-                cudaLaunchConfig_t lc = {};
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = 2;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                lc.blockDim = dim3(kThreads);
-                lc.dynamicSmemBytes = Shape<kPair>::kSmemBytes;
-                lc.stream = stream;
-                lc.attrs = attr;
-                lc.numAttrs = 1;
-                lc.gridDim = dim3(2 * std::max(1, device_sm_count() / 2));
-                int clusters = 0;
-                st = check_cuda(cudaOccupancyMaxActiveClusters(&clusters, tc_sum_kernel<kPair>, &lc),
-                                "cudaOccupancyMaxActiveClusters");
-                if (st != kOk) break;
-                if (clusters < 1) {
-                    st = set_error(kCudaError, "tensor sum: no CTA pair fits on this device");
-                    break;
-                }
-                lc.gridDim = dim3(2 * std::min(a.n_items, clusters));
-                st = check_cuda(cudaLaunchKernelEx(&lc, tc_sum_kernel<kPair>, a), "tc_sum_kernel (pairs) launch");
-                if (st != kOk) break;
+            switch (modes[m]) {
+            case kNarrow: st = launch_tile<kNarrow>(a, stream); break;
+            case kPairNarrow: st = launch_tile<kPairNarrow>(a, stream); break;
+            case kPair: st = launch_tile<kPair>(a, stream); break;
+            default: st = launch_tile<kWide>(a, stream); break;
             }
+            if (st != kOk) break;
             count_launch();
             st = check_cuda(cudaGetLastError(), "tc_sum_kernel launch");
         }

@@ -301,13 +301,13 @@ def test_tensor_form_nyquist_plane(case, grid):
     assert O.rel_l2(spec_tc, spec_pl) < SPEC_TOL
 
 
-@pytest.mark.parametrize("grid", [(64, 64, 64), (64, 64, 144), (256, 256, 160)])
+@pytest.mark.parametrize("grid", [(64, 64, 48), (64, 64, 64), (64, 64, 144), (256, 256, 160)])
 def test_tensor_form_operand_images_match_per_tile_operands(grid):
     """B operands copied from images made once per compute (the default)
     against B operands computed per tile (vis_set_operand_cache_limit(0)), in
-    128x128 tiles (64^3), 128x256 tiles (72 planes) and CTA pairs
-    (256x256x160); a Gaussian and a factored group.  Both paths run the same
-    arithmetic, and both match FP64."""
+    128x128 tiles (24 planes), narrow CTA pairs (64^3: 32 planes), 128x256
+    tiles (72 planes) and CTA pairs (256x256x160); a Gaussian and a factored
+    group.  Both paths run the same arithmetic, and both match FP64."""
     rng = np.random.default_rng(31)
     groups = _tc_groups(rng, 2001)["two_groups"]
     lib = M.lib()
