@@ -1184,8 +1184,10 @@ size_t operand_cache_limit() {
     const long long set = __atomic_load_n(&g_operand_cache_limit, __ATOMIC_RELAXED);
     if (set >= 0) return (size_t)set;
     static const long long env = [] {
+        // unset or negative: the default below (as vis_set_operand_cache_limit(-1))
         const char* e = std::getenv("MV_TC_OPERAND_CACHE_MB");
-        return e ? std::max(0LL, std::atoll(e)) << 20 : -1LL;
+        const long long mb = e ? std::atoll(e) : -1LL;
+        return mb >= 0 ? mb << 20 : -1LL;
     }();
     if (env >= 0) return (size_t)env;
     // an eighth of the device's memory, queried once per device
