@@ -26,11 +26,14 @@
 //     cubic pieces on node-centred cells of width ds (a branch point of the
 //     reference's piecewise definition falls on a cell boundary), built per
 //     launch in FP64 by phi_table_kernel; max error ~1.1e-7 of Phi^(0); terms
-//     beyond the table evaluate the accurate FP32 form directly;
+//     beyond the table (s > 63 for Wendland, > 60 for SPH, where |Phi^| <
+//     1e-11) and terms of negative radii read its last, all-zero cell;
 //   - Gaussians with radii: exp2 per term.
 //
-// Accumulation: each tile's terms are summed in FP32 registers and the tile
-// sums are added with Kahan compensation; splits are reduced in FP64.
+// Accumulation: each tile's terms are summed in FP32 registers; the tile sums
+// go into FP64 running sums in global scratch (folded kernel) or are added
+// with Kahan compensation in registers (unfolded kernel); splits are reduced
+// in FP64.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
