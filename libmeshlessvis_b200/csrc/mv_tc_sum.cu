@@ -38,9 +38,9 @@
 // plain-form pass.
 //
 // CTA tile: M = 128 rows (a, b) (8-row chunks of constant a), N = up to 128 c
-// values (256 real columns: the 128x256 MMA reads A once for twice the work of
-// a 128x128 one, within the shared-memory port), K = 32 particles (64 real)
-// per pipeline stage, 2 stages.
+// values (256 real columns), K = 32 particles (64 real) per pipeline stage;
+// CTA pairs run M = 256 over both CTAs (tile kinds and operand rings at
+// TileMode and Shape below).
 // Warp roles:
 //   warp 0       allocates TMEM, one thread issues tcgen05.mma / commit;
 //   warps 1-4    flush TMEM (warp w reads lanes 32 (w % 4) .. +31);
@@ -67,8 +67,9 @@
 // Every mbarrier wait is bounded (2 s of %globaltimer); a wait that runs out
 // sets *error_flag, raises the CTA's abort flag, and all roles leave their
 // loops; warp 0 drains its MMAs (bounded) before releasing TMEM.  The host
-// reports a non-zero flag at the next synchronising call.  No TMA tensor maps,
-// no clusters, no multicast.
+// reports a non-zero flag at the next synchronising call.  No TMA tensor maps
+// and no multicast loads (only tcgen05.commit signals both CTAs of a pair);
+// clusters of 2 only for the CTA-pair tiles.
 #include <cuda_fp16.h>
 
 #include <algorithm>
