@@ -444,22 +444,21 @@ __device__ __forceinline__ void split_pair(float2 X, float2 Y, uint2& hi, uint2&
     lo = make_uint2(h2_bits(__floats2half2_rn(dx.x, dy.x)), h2_bits(__floats2half2_rn(dx.y, dy.y)));
 }
 
-// One step of both particles' chains: z <- z (R q), then q <- q rho (GAUSS;
-// without it q = 1).  Packed: X' = X Rx - Y Ry, Y' = X Ry + Y Rx; NRY = -RY.
+// One step of both particles' chains: z <- z R, with R = (RX, RY) (NRY =
+// -RY) already scaled by this step's Gaussian ratio; then (GAUSS) R <- R rho
+// for the next step (without GAUSS the ratio is 1).  Packed: X' = X Rx - Y Ry,
+// Y' = X Ry + Y Rx.
 template <bool GAUSS>
-__device__ __forceinline__ void rotate_pair(float2& X, float2& Y, float2 RX, float2 RY, float2 NRY, float2& Q,
-                                            float2 RHO) {
-    float2 rx = RX, ry = RY, nry = NRY;
-    if constexpr (GAUSS) {
-        rx = __fmul2_rn(RX, Q);
-        ry = __fmul2_rn(RY, Q);
-        nry = __fmul2_rn(NRY, Q);
-        Q = __fmul2_rn(Q, RHO);
-    }
-    const float2 nx = __ffma2_rn(X, rx, __fmul2_rn(Y, nry));
-    const float2 ny = __ffma2_rn(X, ry, __fmul2_rn(Y, rx));
+__device__ __forceinline__ void rotate_pair(float2& X, float2& Y, float2& RX, float2& RY, float2& NRY, float2 RHO) {
+    const float2 nx = __ffma2_rn(X, RX, __fmul2_rn(Y, NRY));
+    const float2 ny = __ffma2_rn(X, RY, __fmul2_rn(Y, RX));
     X = nx;
     Y = ny;
+    if constexpr (GAUSS) {
+        RX = __fmul2_rn(RX, RHO);
+        RY = __fmul2_rn(RY, RHO);
+        NRY = __fmul2_rn(NRY, RHO);
+    }
 }
 
 __device__ __forceinline__ uint32_t h2_swap_negate(uint32_t h, bool negate_second) {
@@ -479,6 +478,11 @@ __device__ __forceinline__ int sw_step(int c16, int K) { return K * kRowBytes + 
 template <bool GAUSS, bool UP>
 __device__ __forceinline__ void a_chain(uint8_t* base, int c16, float2 X, float2 Y, float2 RX, float2 RY, float2 NRY,
                                         float2 Q, float2 RHO) {
+    if constexpr (GAUSS) {  // the first step's ratio q0 = Q
+        RX = __fmul2_rn(RX, Q);
+        RY = __fmul2_rn(RY, Q);
+        NRY = __fmul2_rn(NRY, Q);
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         uint8_t* p = base + sw_step(c16, UP ? i : 7 - i);
@@ -486,7 +490,7 @@ __device__ __forceinline__ void a_chain(uint8_t* base, int c16, float2 X, float2
         split_pair(X, Y, hi, lo);
         *reinterpret_cast<uint2*>(p) = hi;
         *reinterpret_cast<uint2*>(p + kABytes) = lo;
-        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
+        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, RHO);
     }
 }
 
@@ -495,6 +499,11 @@ __device__ __forceinline__ void a_chain(uint8_t* base, int c16, float2 X, float2
 template <bool GAUSS>
 __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int lo_gap, int c16, float2 X, float2 Y,
                                         float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
+    if constexpr (GAUSS) {  // the first step's ratio q0 = Q
+        RX = __fmul2_rn(RX, Q);
+        RY = __fmul2_rn(RY, Q);
+        NRY = __fmul2_rn(NRY, Q);
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int off = sw_step(c16, i);
@@ -506,7 +515,7 @@ __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int 
         *reinterpret_cast<uint2*>(im_base + off) = make_uint2(h2_swap_negate(hi.x, false), h2_swap_negate(hi.y, false));
         *reinterpret_cast<uint2*>(im_base + off + lo_gap) =
             make_uint2(h2_swap_negate(lo.x, false), h2_swap_negate(lo.y, false));
-        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, Q, RHO);
+        if (i < 7) rotate_pair<GAUSS>(X, Y, RX, RY, NRY, RHO);
     }
 }
 
