@@ -1197,22 +1197,24 @@ size_t operand_cache_limit() {
         // unset or negative: the default below (as vis_set_operand_cache_limit(-1))
         const char* e = std::getenv("MV_TC_OPERAND_CACHE_MB");
         const long long mb = e ? std::atoll(e) : -1LL;
-        return mb >= 0 ? mb << 20 : -1LL;
+        return mb >= 0 ? std::min(mb, 1LL << 40) << 20 : -1LL;
     }();
     if (env >= 0) return (size_t)env;
-    // an eighth of the device's memory, queried once per device
+    // an eighth of the device's memory, queried once per device (threads that
+    // race here store the same value)
     static size_t total[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-    if (!total[dev]) {
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    size_t t = __atomic_load_n(&total[dev], __ATOMIC_RELAXED);
+    if (!t) {
+        size_t free_b = 0;
+        if (cudaMemGetInfo(&free_b, &t) != cudaSuccess) {
             cudaGetLastError();
             return 0;
         }
-        total[dev] = total_b;
+        __atomic_store_n(&total[dev], t, __ATOMIC_RELAXED);
     }
-    return total[dev] / 8;
+    return t / 8;
 }
 
 extern "C" void vis_set_operand_cache_limit(long long bytes) {
