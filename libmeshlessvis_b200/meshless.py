@@ -19,11 +19,19 @@ __all__ = ["get_simple_meshless_dataset", "delete_meshless_dataset", "delete_mes
            "get_number_of_terms", "load_meshless_datasets_from_file", "save_meshless_datasets_to_file",
            "shift_meshless_dataset", "Dataset", "Config", "Spectrum", "constraints_from_arrays", "VisError",
            "SPH", "GAUSSIAN", "WENDLAND_D3_C2", "GAUSSIAN_DECAYING", "FORM_AUTO", "FORM_PLAIN", "FORM_TENSOR",
-           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT", "STAGE_TENSOR_SUM", "Batch"]
+           "STAGE_SUM", "STAGE_SLICE", "STAGE_FFT", "STAGE_TENSOR_SUM", "Batch", "set_operand_cache_limit"]
 
 
 def lib():
     return L.load()
+
+
+def set_operand_cache_limit(nbytes):
+    """Device memory the tensor form may keep as precomputed B operands
+    (vis_set_operand_cache_limit): None restores the default (an eighth of
+    device memory, or MV_TC_OPERAND_CACHE_MB), 0 turns them off.  Applies to
+    later computes in this process."""
+    lib().vis_set_operand_cache_limit(-1 if nbytes is None else max(0, int(nbytes)))
 
 
 def constraints_from_arrays(positions, weights):

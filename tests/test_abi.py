@@ -183,3 +183,13 @@ def test_autotune_table_starts_with_the_defaults():
     tuned = lib.vis_autotune_lookup(L.int3(64, 64, 64), 4096, 2, 0, *[ctypes.byref(v) for v in vals])
     assert tuned == 0
     assert [v.value for v in vals] == [6, 4, 16]
+
+
+def test_operand_cache_limit_setter_takes_every_form():
+    """The operand-cache limit is a process-wide setting that needs no GPU to
+    set: a byte count, 0 (off), and None / negative (the default)."""
+    M.set_operand_cache_limit(0)
+    M.set_operand_cache_limit(3 << 30)
+    M.set_operand_cache_limit(None)
+    L.load().vis_set_operand_cache_limit(-5)
+    M.set_operand_cache_limit(None)
