@@ -2,13 +2,16 @@
 """Benchmark of the libMeshlessVis hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c3] [--form auto|plain|tensor]
+                    [--workload c3|c1|c2|c4|c5|...] [--form auto|plain|tensor]
+                    [--no-compare-forms]
 
 One step = one pass of the hot path over one particle set resident in HBM:
 the 3D half-spectrum Fourier sum of every group, then slice extraction and
-batched 2D C2R of all the workload's views.  Default workload: C2 (N=262,144
-Plummer particles, 32-NN weights and radii, Wendland D3 C2, 128x128x65
-half-spectrum, 64 views rotating about y, 128^2 images).
+batched 2D C2R of all the workload's views.  Default workload: C3, the
+precision-form configuration (N=2^20 uniform particles, w ~ U(0,1),
+GAUSSIAN_DECAYING with h log-uniform in [0.005, 0.05] in 16 h-bins, 256x256x129
+half-spectrum, one z-normal view at 256^2), with the spectrum sum also timed
+alone in the tensor-core form and in the plain FP32 form (tc_vs_plain).
 
 Prints one JSON line (rank 0).  value = particle x frequency terms per second
 over the whole step (GTerms/s), device time by CUDA events on the library's
@@ -64,31 +67,43 @@ def sum_terms_split(w):
     return plane * (lz_tc + (1 if nyq_tc else 0)), (0 if nyq_tc else plane)
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from ncu
+# captures of dram__bytes_read.sum + dram__bytes_write.sum (profiles/*.md
+# names the capture and its command); None where no capture exists.
+DRAM_TRAFFIC_PER_LAUNCH = {}
+
+
 def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
     """Roofline of the dominant Fourier-sum kernel: 8 algorithmic flops per
-    particle x frequency term over the kernel's own event-timed duration."""
+    particle x frequency term over the kernel's own event-timed duration.  The
+    tensor kernel runs back to back inside a long step, so its denominator is
+    the sustained dense bf16 figure (the FP16 dense rate is the same)."""
     terms, n, g = terms_per_step(w)
     (p_ms, p_n), (t_ms, t_n) = stage_t[0], stage_t[3]
     max_mhz = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    traffic = DRAM_TRAFFIC_PER_LAUNCH.get(w["name"])
     if t_ms > p_ms and t_n > 0:
         tc_terms, _ = sum_terms_split(w)
         per_launch_terms = tc_terms * steps / t_n
         launch_s = t_ms / t_n / 1000.0
         alg = 8.0 * per_launch_terms / launch_s / 1e12
         issued = 24.0 * per_launch_terms / launch_s / 1e12
-        peak = peaks.get("bf16_tflops", 1590.0)
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        burst = peaks.get("bf16_tflops", 1590.0)
         return {"bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak,
-                "traffic": None, "kernel": "tc_sum_kernel", "flops_per_term": 8,
-                "issued_tflops": issued, "issued_frac": issued / peak,
+                "traffic": traffic, "kernel": "tc_sum_kernel", "flops_per_term": 8,
+                "issued_tflops": issued, "issued_frac": issued / peak, "issued_frac_of_burst": issued / burst,
                 "issued_note": "3 FP16 products per term (hi*hi, hi*lo, lo*hi): 24 issued flops per term",
-                "launch_ms": t_ms / t_n, "launches": t_n,
-                "peak_source": f"{peak_src} dense bf16 cuBLAS burst (FP16 dense rate is the same on B200)"}
+                "terms_per_launch": per_launch_terms, "launch_ms": t_ms / t_n, "launches": t_n,
+                "peak_source": f"{peak_src} dense bf16 cuBLAS, sustained (the kernel runs back to back inside a "
+                               f"long step; burst {burst})"}
     per_launch_terms = terms * steps / max(1, p_n)
     launch_s = p_ms / max(1, p_n) / 1000.0
     alg = 8.0 * per_launch_terms / launch_s / 1e12 if launch_s > 0 else 0.0
     peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
-    r = {"bound": "fp32", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak, "traffic": None,
-         "kernel": "plain_sum_kernel", "flops_per_term": 8, "launch_ms": p_ms / max(1, p_n), "launches": p_n,
+    r = {"bound": "fp32", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak, "traffic": traffic,
+         "kernel": "fold_sum_kernel", "flops_per_term": 8, "terms_per_launch": per_launch_terms,
+         "launch_ms": p_ms / max(1, p_n), "launches": p_n,
          "peak_source": f"nominal FP32: {sm_count} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x {max_mhz:.0f} MHz "
                         "(MEASURED_PEAKS.json has no FP32 figure)"}
     if clk.get("sm_mhz"):
@@ -144,16 +159,18 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c3w", "c4", "c5"], default="c2",
+    p.add_argument("--workload", choices=["c1", "c2", "c2s", "c3", "c3s", "c3w", "c4", "c5", "c5s"], default="c3",
                    help="c2s: C2's particle model at N=65,536 on a 64^3 lattice, 16 views; c3s: C3's model at "
-                        "N=2^17, 128^3, 4 h-bins; c3w: the same on 256^3 (the 128x256 tensor tile) (profiling cases)")
+                        "N=2^17, 128^3, 4 h-bins; c3w: the same on 256^3; c5s: C5's model at N=2^17 on its 384^3 "
+                        "lattice, 8 views (profiling cases)")
     p.add_argument("--form", choices=["auto", "plain", "tensor"], default="auto")
     p.add_argument("--autotune", action="store_true",
                    help="run the library's autotuner (vis_autotune_spectrum) on the workload before the warm-up")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--compare-forms", action="store_true",
-                   help="also time the spectrum sum alone in the tensor and the plain form (tc_vs_plain)")
+    p.add_argument("--no-compare-forms", dest="compare_forms", action="store_false",
+                   help="skip timing the spectrum sum alone in the tensor and the plain form (tc_vs_plain; on by "
+                        "default)")
     return p.parse_args()
 
 
@@ -178,6 +195,13 @@ def workload(name):
     if name == "c2s":
         w = W.c2(n=65536, grid=64, views=16)
         w["name"] = "C2-small"
+        return w
+    if name == "c5s":
+        # C5's lattice and tile (384^3: CTA pairs with n-tiles of 96 + 96 c
+        # values) and its particle model at N=2^17, for profiling
+        w = next(W.c5_frames(n=1 << 17, frames=1))
+        w["name"] = "C5-small"
+        w["views"] = w["views"][:8]
         return w
     return W.c2()
 
@@ -260,36 +284,64 @@ def reference_groups(groups):
     return out, note
 
 
-def cpu_baseline(w, target_terms=6e9):
-    """The reference's own fourier_transform (OpenMP, all host threads) on the
-    workload's particles, for one slice of 2*cx*cy frequencies, cx = cy chosen
-    so the sample is about target_terms terms (at most 64)."""
+# The reference's CPU loop hands out block_length frequencies at a time to its
+# OpenMP threads (schedule(dynamic, block_length),
+# meshless_vis/fourier_transform_cpu.cpp:85); 32 is its smallest supported
+# block length (fourier_transform_cpu.cpp:159-163).
+REF_BLOCK_LENGTH = 32
+REF_MIN_CHUNKS_PER_THREAD = 4
+
+
+def reference_sample(n, cores, target_terms=2e9):
+    """The slice the reference's CPU path is timed on: all n particles over one
+    z-normal slice of 2*c*c frequencies, c chosen so the sample holds about
+    target_terms terms (at most c = 64) but never fewer than
+    REF_MIN_CHUNKS_PER_THREAD chunks of REF_BLOCK_LENGTH frequencies for every
+    host thread.  Returns (c, block_length)."""
+    c_min = int(np.ceil((REF_MIN_CHUNKS_PER_THREAD * REF_BLOCK_LENGTH * max(1, cores) / 2.0) ** 0.5))
+    c = int(max(4, min(64, (target_terms / (2.0 * max(1, n))) ** 0.5)))
+    return max(c, c_min), REF_BLOCK_LENGTH
+
+
+def reference_timer(groups, cores, target_terms=2e9):
+    """(fn, terms, kind, sample text, close): one call of fn runs the
+    reference's own fourier_transform (OpenMP, all host threads) over the
+    sample of reference_sample; without oracle/_ref the FP64 oracle's C slice
+    sum (kind "port") stands in."""
     import oracle as O
 
-    groups = w["groups"]
     n = sum(len(c) for c, _, _ in groups)
-    c = int(max(4, min(64, (target_terms / (2.0 * max(1, n))) ** 0.5)))
-    cx, cy = c, c
-    terms = n * 2 * cx * cy
-    cores = len(os.sched_getaffinity(0))
+    c, bl = reference_sample(n, cores, target_terms)
+    terms = n * 2 * c * c
     note = ""
     if O.ref_available():
         ref_groups, note = reference_groups(groups)
-        R = O.RefRenderer(ref_groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
-        t0 = time.perf_counter()
-        R.fourier_transform()
-        dt = time.perf_counter() - t0
-        R.close()
-        kind = "reference"
+        R = O.RefRenderer(ref_groups, (1.0, 1.0), (c, c), (1, 0, 0), (0, 1, 0), (2 * c, 2 * c), block_length=bl)
+        fn, close, kind = R.fourier_transform, R.close, "reference"
     else:
-        t0 = time.perf_counter()
-        for cons, radii, basis in groups:
-            O.slice_sum(cons, radii, basis, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0))
-        dt = time.perf_counter() - t0
-        kind = "port"
+        def fn():
+            for cons, radii, basis in groups:
+                O.slice_sum(cons, radii, basis, (1.0, 1.0), (c, c), (1, 0, 0), (0, 1, 0))
+
+        close, kind = (lambda: None), "port"
+    chunks = 2 * c * c // bl
+    sample = (f"the reference's fourier_transform (OpenMP, {cores} threads, block_length {bl}: {chunks} chunks, "
+              f"{chunks / max(1, cores):.1f} per thread) over all {n} particles and one z-normal slice of "
+              f"2*{c}*{c}={2 * c * c} frequencies ({terms:.3e} terms){note}")
+    return fn, terms, kind, sample, close
+
+
+def cpu_baseline(w, target_terms=2e9):
+    """The reference's own fourier_transform on the workload's particles, one
+    call over the reference_sample slice, timed on the host."""
+    cores = len(os.sched_getaffinity(0))
+    fn, terms, kind, sample, close = reference_timer(w["groups"], cores, target_terms)
+    t0 = time.perf_counter()
+    fn()
+    dt = time.perf_counter() - t0
+    close()
     return {"value": terms / dt / 1e9, "unit": "GTerms/s", "cores": cores, "kind": kind,
-            "sample": f"reference fourier_transform (direct slice sum) of all {n} particles over one z-normal "
-                      f"slice of 2*{cx}*{cy}={2 * cx * cy} frequencies ({terms:.3e} terms, {dt:.2f} s){note}"}
+            "sample": f"{sample}, {dt:.2f} s"}
 
 
 def accuracy_check(w, spec, images, n_points=1024, n_views=2):
@@ -333,30 +385,20 @@ def run_reference(args):
         w = dict(max(W.c4(), key=lambda x: sum(len(c) for c, _, _ in x["groups"])), name="C4 (largest set)")
     else:
         w = workload(args.workload)
-    cx, cy = (32, 32)
     groups = w["groups"]
     n = sum(len(c) for c, _, _ in groups)
-    terms = n * 2 * cx * cy
     cores = len(os.sched_getaffinity(0))
-    kind = "reference" if O.ref_available() else "port"
-    note = ""
-    if kind == "reference":
-        ref_groups, note = reference_groups(groups)
-        R = O.RefRenderer(ref_groups, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0), (2 * cx, 2 * cy))
-        fn = R.fourier_transform
-    else:
-        def fn():
-            for cons, radii, basis in groups:
-                O.slice_sum(cons, radii, basis, (1.0, 1.0), (cx, cy), (1, 0, 0), (0, 1, 0))
+    fn, terms, kind, sample, close = reference_timer(groups, cores)
     for _ in range(args.warmup):
         fn()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         fn()
     dt = time.perf_counter() - t0
+    close()
     value = terms * args.steps / dt / 1e9
-    sample = (f"per step: the reference's fourier_transform (OpenMP, {cores} threads) over all {n} particles of "
-              f"workload {w['name']} and one slice of {2 * cx * cy} frequencies ({terms:.3e} terms){note}")
+    sample = f"per step, workload {w['name']}: {sample}"
+    n_freq = terms // max(1, n)
     kx, ky, kz = w["grid"]
     # our arm's metric and workload keys; the reference's rate per term is
     # timed on one slice of the same particles (it cannot offset k_z)
@@ -365,11 +407,9 @@ def run_reference(args):
             "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w["name"], "particles": n, "grid": [kx, ky, kz],
-                       "half_spectrum": kx * ky * (kz // 2 + 1), "sample_frequencies": 2 * cx * cy},
+                       "half_spectrum": kx * ky * (kz // 2 + 1), "sample_frequencies": int(n_freq)},
             "cpu_baseline": {"value": value, "unit": "GTerms/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "GTerms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if kind == "reference":
-        R.close()
     print(json.dumps(line), flush=True)
 
 
@@ -554,11 +594,42 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def batch_accuracy(sets, batch, picks, n_points=256, n_views=1):
+    """The oracle as the checker of a batch run: for the picked jobs, the FP64
+    direct sum at seeded half-spectrum points against the job's spectrum, and
+    FP64 slice extraction + C2R of that spectrum against its first views."""
+    import oracle as O
+
+    prng = np.random.default_rng(1)
+    got_all, ref_all, img_err = [], [], []
+    t0 = time.perf_counter()
+    for j in picks:
+        w = sets[j]
+        kx, ky, kz = w["grid"]
+        ijk = np.stack([prng.integers(-kx // 2, kx // 2, n_points), prng.integers(-ky // 2, ky // 2, n_points),
+                        prng.integers(0, kz // 2 + 1, n_points)], axis=1).astype(np.int32)
+        spec = batch.spectrum(j)
+        ref = sum(O.spectrum_points(c, r, b, w["step3"], ijk) for c, r, b in w["groups"])
+        got_all.append(spec[ijk[:, 0] + kx // 2, ijk[:, 1] + ky // 2, ijk[:, 2]])
+        ref_all.append(ref)
+        imgs = batch.images(j)[:n_views]
+        ref_img = O.render_from_spectrum(spec.astype(np.complex128), w["grid"], w["step3"], w["step"], w["cutoff"],
+                                         w["views"][:n_views], w["samples"])
+        img_err.append(O.rel_l2(imgs, ref_img))
+    got, ref = np.concatenate(got_all), np.concatenate(ref_all)
+    return {"spectrum": {"rel_l2": O.rel_l2(got, ref), "max_abs_over_max": O.max_abs(got, ref) / np.max(np.abs(ref)),
+                         "points": int(len(got)), "jobs": [int(j) for j in picks], "tolerance": 1e-5,
+                         "oracle": "FP64 direct sum", "seconds": round(time.perf_counter() - t0, 2)},
+            "images": {"rel_l2": max(img_err), "views_per_job": n_views, "tolerance": 1e-4,
+                       "oracle": "FP64 slice interpolation + C2R of the same spectrum (worst job)"}}
+
+
 def run_batch(args):
     """C4: 64 particle sets of uneven size and lattice, 16 views each, as one
     batch (one CUDA graph per execute)."""
     import torch
 
+    from libmeshlessvis_b200 import _lib as L
     from libmeshlessvis_b200 import meshless as M
     from libmeshlessvis_b200 import workloads as W
 
@@ -580,20 +651,28 @@ def run_batch(args):
     stream = torch.cuda.Stream()
     cfg.set_stream(stream.cuda_stream)
     terms = 0
+    tc_terms = 0
     n_total = 0
     n_views = 0
     datasets = []
     batch = M.Batch(cfg)
+
+    def add_all(b, dss):
+        for ds, w in zip(dss, sets):
+            b.add(ds, w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], [v[0] for v in w["views"]],
+                  [v[1] for v in w["views"]])
+
     for w in sets:
+        w["name"] = "C4-set"
         ds = M.Dataset(w["groups"])
         cfg.register(ds)
         datasets.append(ds)
         t, n, g = terms_per_step(w)
         terms += t
+        tc_terms += sum_terms_split(w)[0]
         n_total += n
         n_views += len(w["views"])
-        batch.add(ds, w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], [v[0] for v in w["views"]],
-                  [v[1] for v in w["views"]])
+    add_all(batch, datasets)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(max(3, args.warmup)):
         batch.execute(form)
@@ -624,18 +703,92 @@ def run_batch(args):
     per_exec = launches_host / max(1, args.steps)
     if uses_graph == 1:
         probe = M.Batch(cfg)
-        for ds, w in zip(datasets, sets):
-            probe.add(ds, w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], [v[0] for v in w["views"]],
-                      [v[1] for v in w["views"]])
+        add_all(probe, datasets)
         c0 = lib.vis_kernel_launch_count()
         probe.execute(form)  # builds: one direct run + one capture of the same sequence
         per_exec = (lib.vis_kernel_launch_count() - c0) / 2
         probe.close()
+    accuracy = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the largest, the smallest and two middle sets (outside the timed region)
+        order = np.argsort([sum(len(c) for c, _, _ in w["groups"]) for w in sets])
+        picks = sorted({int(order[-1]), int(order[0]), int(order[len(order) // 2]), int(order[len(order) // 4])})
+        accuracy = batch_accuracy(sets, batch, picks)
+    # end to end: every step registers all sets from pinned host memory,
+    # executes the batch, copies every job's images to the host and unregisters
+    e2e = None
+    if not args.no_e2e:
+        groups_h, pinned, h2d = [], [], 0
+        for w in sets:
+            gs = []
+            for cons, radii, basis in w["groups"]:
+                tc = torch.empty(len(cons) * 16, dtype=torch.uint8, pin_memory=True)
+                pc = tc.numpy().view(cons.dtype)
+                pc[:] = cons
+                tr = torch.empty(len(radii), dtype=torch.float32, pin_memory=True)
+                pr = tr.numpy()
+                pr[:] = radii
+                pinned += [tc, tr]
+                h2d += pc.nbytes + pr.nbytes
+                gs.append((pc, pr, basis))
+            groups_h.append(gs)
+        h_imgs = [torch.empty((len(w["views"]),) + tuple(w["samples"]), dtype=torch.float32, pin_memory=True)
+                  for w in sets]
+        d2h = sum(t.numel() * 4 for t in h_imgs)
+        ds2 = [M.Dataset(gs) for gs in groups_h]
+        b2 = M.Batch(cfg)
+        add_all(b2, ds2)
+
+        def e2e_step():
+            for d in ds2:
+                cfg.register(d)
+            b2.execute(form)
+            for j, t in enumerate(h_imgs):
+                L.check(lib, lib.vis_batch_copy_images_to_host(b2.ptr, j, t.data_ptr()))
+            for d in ds2:
+                cfg.unregister(d)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                e_ev[k][0].record(stream)
+                e2e_step()
+                e_ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e_ev), dist, "cuda")
+        e2e = {"value": world * terms * args.steps / (e_ms / 1000.0) / 1e9, "unit": "GTerms/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms / args.steps,
+               "wall_ms_per_step": wall * 1000 / args.steps, "cuda_graph": b2.uses_graph()}
+        b2.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        big = max(sets, key=lambda x: sum(len(c) for c, _, _ in x["groups"]))
+        cpu = cpu_baseline(big)
+        cpu["sample"] = "largest set of the batch: " + cpu["sample"]
     batch.close()
     for ds in datasets:
         cfg.unregister(ds)
     cfg.close()
     if rank == 0:
+        peaks, peak_src = measured_peaks()
+        # the batch runs as one CUDA graph, whose launches the library's stage
+        # timer cannot see: the step time bounds the tensor kernel's time
+        alg = 8.0 * tc_terms * args.steps / (t_max / 1000.0) / 1e12
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        roofline = {"bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak,
+                    "traffic": None, "kernel": "tc_sum_kernel", "flops_per_term": 8,
+                    "issued_tflops": 3 * alg, "issued_frac": 3 * alg / peak,
+                    "timing": "whole-step CUDA-event time (graph replay: every kernel of the step included), so "
+                              "achieved is a lower bound for the tensor kernel",
+                    "peak_source": f"{peak_src} dense bf16 cuBLAS, sustained"}
         line = {"metric": METRIC_BATCH,
                 "value": value, "unit": "GTerms/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -645,7 +798,14 @@ def run_batch(args):
                            "l2": "flushed between timed steps (256 MB write outside the event pair)",
                            "parallelism": f"replicas x{world}"},
                 "views_per_s": replica_throughput(n_views, args.steps, t_max, world),
-                "clocks": clk, "gpu_launches": int(round(per_exec * args.steps))}
+                "roofline": roofline, "clocks": clk, "gpu_launches": int(round(per_exec * args.steps)),
+                "peaks_source": peak_src}
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if accuracy:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

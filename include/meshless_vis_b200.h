@@ -126,6 +126,20 @@ void vis_autotune_clear(void);
  * Process-wide; applies to later computes.  No counterpart in the reference. */
 void vis_set_operand_cache_limit(long long bytes);
 
+/* For tests of the tensor form's failure path (no counterpart in the
+ * reference).  Every mbarrier wait of the tensor-core kernel is bounded (2 s);
+ * a wait that runs out sets a device error word, the kernel's CTAs leave their
+ * loops, release their tensor memory and return, and the next synchronising
+ * call on the config (vis_config_synchronize, vis_spectrum_copy_to_host, ...)
+ * returns VIS_ERROR_CUDA with a message naming the wait.  This hook makes the
+ * NEXT tensor-core launch of the process (one shot) bound its waits by
+ * wait_limit_ns (1e5 .. 2e9) and withhold one arrival on its first pipeline
+ * stage, so that the MMA thread's first wait runs out before any MMA is
+ * issued.  Nothing faults; the device stays usable and later computes are
+ * unaffected.  That compute's results are invalid.  Returns VIS_SUCCESS or
+ * VIS_ERROR_INVALID_VALUE. */
+int vis_tensor_wait_test_hook(long long wait_limit_ns);
+
 /* ------------------------------------------------------------------ batch */
 /* A batch of jobs, each one registered dataset with its own half-spectrum
  * lattice and its own views and image size (the reference renders one view of
@@ -217,8 +231,12 @@ unsigned long long vis_kernel_launch_count(void);
  * is a fixed 8 MiB array in the library's device image, which every GPU that
  * loads the library holds until the process exits; slices of more than about
  * 1.04 million samples are rejected with VIS_ERROR_INVALID_VALUE.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  All calls share the one
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and keeps it for the life of the process, so make that first call before any
+ * stream capture; the kept address does not survive a cudaDeviceReset of that
+ * device, after which this entry point must not be called.  Groups with SPH or
+ * Wendland radii build a 4097-cell Phi^ table per call (64 KiB of shared
+ * memory), since no radius maximum is known here.  All calls share the one
  * array: calls whose work overlaps on the GPU (different streams, or different
  * host threads on one device) race and must be serialised by the caller.
  * Returns VIS_SUCCESS or a VisError code. */

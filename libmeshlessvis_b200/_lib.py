@@ -111,6 +111,7 @@ SIGNATURES = {
     "vis_autotune_lookup": (c_int, [int3, c_longlong, c_int, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
     "vis_autotune_clear": (None, []),
     "vis_set_operand_cache_limit": (None, [ctypes.c_longlong]),
+    "vis_tensor_wait_test_hook": (c_int, [ctypes.c_longlong]),
     "vis_spectrum_copy_to_host": (c_int, [c_void_p, PConfig, c_void_p]),
     "vis_spectrum_render_views": (c_int, [c_void_p, PConfig, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "vis_config_enable_kernel_timing": (c_int, [PConfig, c_int]),

@@ -73,6 +73,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -117,6 +118,10 @@ constexpr int kDumpFlushes = 16;  // chain partials summed in FP32 before an FP6
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
 constexpr float kInvProductScale = 1.f / (4096.f * 4096.f);  // 2^-24
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+// After a wait has run out, a CTA idles this long before it releases TMEM and
+// exits, so bulk copies it issued (which complete within microseconds) have
+// landed in its shared memory.
+constexpr unsigned long long kAbortGraceNs = 200000ull;
 
 // Tile kinds (template parameter MODE):
 //   kNarrow (lattices with at most 64 tensor planes): 128x128 MMA, two
@@ -183,6 +188,8 @@ struct TcArgs {
     int n_items;
     int flush_stages;  // stages per TMEM accumulation chain (12 MMAs each)
     int* error_flag;
+    unsigned long long wait_limit_ns;  // bound of every mbarrier wait (kWaitLimitNs unless a test shortens it)
+    int withhold_first_arrival;        // test hook: CTA 0's loader skips its arrival on the first full barrier
 };
 
 // Work of one item as every role sees it.
@@ -297,13 +304,13 @@ __device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t pa
 constexpr uint32_t kSuspendHintNs = 100000;  // 0.1 ms per suspension; the phase's completion wakes the thread first
 
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* error_flag,
-                                          int code) {
+                                          unsigned long long limit_ns, int code) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     while (true) {
         if (*abort_flag) return false;
         if (mbar_try_wait_suspend(bar, parity, kSuspendHintNs)) return true;
-        if (global_ns() - t0 > kWaitLimitNs) {
+        if (global_ns() - t0 > limit_ns) {
             *abort_flag = 1;
             atomicOr(error_flag, code);
             return false;
@@ -658,8 +665,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     const int b = k % kBufs, u = k / kBufs;  // accumulator and its use count
                     const bool first = (s % flush_stages) == 0;
                     // a chain starts once the flush of the accumulator's previous chain has read it
-                    if (first && u >= 1 && !mbar_wait(&acc_empty[b], (u - 1) & 1, abort_flag, a.error_flag, 1)) break;
-                    if (!mbar_wait(&full[fb], (S / kFull) & 1, abort_flag, a.error_flag, 2)) break;
+                    if (first && u >= 1 && !mbar_wait(&acc_empty[b], (u - 1) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 1)) break;
+                    if (!mbar_wait(&full[fb], (S / kFull) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 2)) break;
                     tc_fence_after();
                     const uint32_t a_hi = smem_u32(a_ring + ab * SH::kAStageBytes), a_lo = a_hi + kABytes;
                     // B: hi rows, then lo rows (2 bnc rows each)
@@ -694,7 +701,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     int s = 0;
                     for (; s < I.n_stages; ++s, ++S) {
                         const int fb = S % kFull;
-                        if (!mbar_wait(&pfull[fb], (S / kFull) & 1, abort_flag, a.error_flag, 256)) break;
+                        if (!mbar_wait(&pfull[fb], (S / kFull) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 256)) break;
                         mbar_arrive_leader(&full[fb]);
                     }
                     if (s < I.n_stages) break;
@@ -725,7 +732,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 const int b = k % kBufs, u = k / kBufs;
                 const uint32_t acc_col = lane_base + (uint32_t)(b * SH::kN);
                 // warp-uniform outcome: the warp arrives as one below
-                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, 4))) break;
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, a.wait_limit_ns, 4))) break;
                 tc_fence_after();
                 tmem_wait_st();  // the previous flush's stores of the total
                 // chain partials are summed in FP32 for kDumpFlushes chains, then
@@ -794,7 +801,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 for (int s = 0; s < I.n_stages; ++s, ++S) {
                     const int buf = S % kSlots;
                     // this CTA's producers have read the slot's constants of stage S - kSlots
-                    if (S >= kSlots && !mbar_wait(&sfree[buf], ((S / kSlots) - 1) & 1, abort_flag, a.error_flag, 32))
+                    if (S >= kSlots && !mbar_wait(&sfree[buf], ((S / kSlots) - 1) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 32))
                         break;
                     const int block = I.kb / kBlockParticles + s;
                     mbar_arrive_expect_tx(&pdata[buf], kBlockBytes);
@@ -814,8 +821,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 int s = 0;
                 for (; s < I.n_stages; ++s, ++S) {
                     const int bb = S % kBStages;
-                    if (!mbar_wait(&b_empty[bb], ((S / kBStages) & 1) ^ 1, abort_flag, a.error_flag, 512)) break;
+                    if (!mbar_wait(&b_empty[bb], ((S / kBStages) & 1) ^ 1, abort_flag, a.error_flag, a.wait_limit_ns, 512)) break;
                     uint64_t* fb = rank == 0 ? &full[S % kFull] : &pfull[S % kFull];
+                    // test hook (vis_tensor_wait_test_hook): the first stage of
+                    // the launch's first unit never completes, so the MMA's
+                    // first wait runs out before any MMA is issued
+                    if (a.withhold_first_arrival && S == 0 && unit == 0 && rank == 0) continue;
                     if (I.bimg) {
                         const int block = I.kb / kBlockParticles + s;
                         mbar_arrive_expect_tx(fb, (uint32_t)I.img_bytes);
@@ -848,7 +859,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             const int b_s = a_up ? b0 : b0 + 7;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
                 const int buf = S % kSlots;
-                if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kSlots) & 1, abort_flag, a.error_flag, 64)))
+                if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kSlots) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 64)))
                     break;
                 uint32_t pqx[2], pqy[2], pqz[2];
                 float pamp[2], pgam[2], prho2[2];
@@ -894,9 +905,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 if (lane == 0) mbar_arrive(&sfree[buf]);
                 // the ring buffer this warp writes: A or B
                 const bool waited = has_a ? mbar_wait(&a_empty[S % kAStages], ((S / kAStages) & 1) ^ 1, abort_flag,
-                                                      a.error_flag, 8)
+                                                      a.error_flag, a.wait_limit_ns, 8)
                                           : mbar_wait(&b_empty[S % kBStages], ((S / kBStages) & 1) ^ 1, abort_flag,
-                                                      a.error_flag, 8);
+                                                      a.error_flag, a.wait_limit_ns, 8);
                 if (!__all_sync(0xffffffffu, waited)) break;
                 uint8_t* st = has_a ? a_ring + (S % kAStages) * SH::kAStageBytes
                                     : b_ring + (S % kBStages) * SH::kBStageBytes;
@@ -969,6 +980,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
     }
 
     // ------------------------------------------------------------- teardown
+    // a CTA that gave up a wait may still have bulk copies in flight into its
+    // shared memory: give them time to land before anything is released
+    if (tid == 0 && *abort_flag) {
+        const unsigned long long t0 = global_ns();
+        while (global_ns() - t0 < kAbortGraceNs) {
+        }
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -1187,6 +1205,8 @@ int tc_flush_stages(int mode) {
 constexpr int kImageMinReuse = 4;
 
 long long g_operand_cache_limit = -1;  // bytes; -1: the default policy
+// Set by vis_tensor_wait_test_hook; taken by the next tensor launch (one shot).
+std::atomic<long long> g_test_wait_limit_ns{0};
 
 }  // namespace
 
@@ -1215,6 +1235,13 @@ size_t operand_cache_limit() {
         __atomic_store_n(&total[dev], t, __ATOMIC_RELAXED);
     }
     return t / 8;
+}
+
+extern "C" int vis_tensor_wait_test_hook(long long wait_limit_ns) {
+    if (wait_limit_ns < 100000LL || wait_limit_ns > (long long)kWaitLimitNs)
+        return set_error(kInvalidValue, "vis_tensor_wait_test_hook: limit outside [1e5, 2e9] ns");
+    g_test_wait_limit_ns.store(wait_limit_ns);
+    return kOk;
 }
 
 extern "C" void vis_set_operand_cache_limit(long long bytes) {
@@ -1556,6 +1583,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
                                (int)plan.items.size() - plan.n_narrow - plan.n_pair_narrow - plan.n_pair};
         const int modes[4] = {kNarrow, kPairNarrow, kPair, kWide};
         int first = 0;
+        bool hooked = false;
         for (int m = 0; m < 4 && st == kOk; first += counts[m], ++m) {
             TcArgs a;
             a.jobs = static_cast<const TcJob*>(plan.d_jobs);
@@ -1563,7 +1591,17 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             a.n_items = counts[m];
             a.flush_stages = narrow_mode(modes[m]) ? plan.flush_narrow : plan.flush;
             a.error_flag = error_flag;
+            a.wait_limit_ns = kWaitLimitNs;
+            a.withhold_first_arrival = 0;
             if (a.n_items == 0) continue;
+            if (!hooked) {
+                hooked = true;
+                const long long t = g_test_wait_limit_ns.exchange(0);
+                if (t > 0) {
+                    a.wait_limit_ns = (unsigned long long)t;
+                    a.withhold_first_arrival = 1;
+                }
+            }
             switch (modes[m]) {
             case kNarrow: st = launch_tile<kNarrow>(a, stream); break;
             case kPairNarrow: st = launch_tile<kPairNarrow>(a, stream); break;

@@ -49,7 +49,7 @@ def direct_cases():
         add(f"b{basis}_noradii", [(constraints(pos * 20, w), None, basis)], (0.05, 0.05), (16, 16), (1, 0, 0),
             (0, 1, 0), (32, 32))
     # two groups, different bases, step 0.1 on shifted positions (the headless
-    # renderer shifts by -5, vis_noninteractive/main.cpp:327)
+    # renderer shifts by -5, vis_noninteractive/main.cpp:46)
     p1 = rng.random((300, 3), dtype=np.float32) * 10 - 5
     p2 = rng.random((200, 3), dtype=np.float32) * 10 - 5
     g1 = (constraints(p1, rng.random(300, dtype=np.float32)), np.full(300, 0.4, np.float32), O.SPH)

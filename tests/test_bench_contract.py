@@ -63,3 +63,18 @@ def test_term_split_follows_the_tensor_plan():
     # Kx/2 = 20 is no multiple of 16 on CTA pairs: the Nyquist plane stays plain
     tc, plain = bench.sum_terms_split(_w((40, 256, 160)))
     assert tc == 10 * 40 * 256 * 80 and plain == 10 * 40 * 256
+
+
+def test_reference_sample_gives_every_thread_four_chunks():
+    """The reference's loop hands out block_length frequencies at a time
+    (schedule(dynamic, block_length), fourier_transform_cpu.cpp:85); the timed
+    slice gives every host thread at least four such chunks, so no core idles
+    and the reference arm and the GPU arm's cpu_baseline time the same sample."""
+    for cores in (1, 2, 8, 16, 64, 192):
+        for n in (4096, 262144, 1 << 20, 1 << 24):
+            c, bl = bench.reference_sample(n, cores)
+            assert bl == bench.REF_BLOCK_LENGTH == 32
+            assert (2 * c * c) // bl >= 4 * cores
+            assert c >= 4
+    # C3 on a 16-thread host: one 64x32 slice (2048 frequencies, 64 chunks)
+    assert bench.reference_sample(1 << 20, 16) == (32, 32)
