@@ -85,6 +85,54 @@ GroupStats registered_group_stats(const void* d_constraints) {
     return it == g_stats.end() ? GroupStats{} : it->second;
 }
 
+// kHBinFine + 1 log-spaced edges from h_min to h_max, as floats: the same
+// computation every time for the same (h_min, h_max).
+std::vector<float> hbin_fine_edges(float h_min, float h_max) {
+    std::vector<float> e(kHBinFine + 1);
+    const double l0 = std::log((double)h_min), l1 = std::log((double)h_max);
+    for (int i = 0; i <= kHBinFine; ++i) e[i] = (float)std::exp(l0 + (l1 - l0) * (double)i / kHBinFine);
+    return e;
+}
+
+// Largest i with edges[i] <= h, clamped to [0, kHBinFine) (float comparisons
+// only: the device scatter classifies the same way against the same floats).
+int hbin_fine_index(const std::vector<float>& edges, float h) {
+    int lo = 0, hi = kHBinFine;  // edges[lo] <= h < edges[hi] once narrowed
+    if (!(h >= edges[1])) return 0;
+    if (h >= edges[kHBinFine - 1]) return kHBinFine - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (edges[mid] <= h) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+namespace {
+std::atomic<unsigned long long> g_hbin_ids{0};
+
+// The smoothing-length histogram of a group whose Phi^ does not separate per
+// axis (SPH, WENDLAND_D3_C2) with varying radii; null otherwise.
+std::shared_ptr<const HBinStats> hbin_histogram(const Group& grp, const GroupStats& gs) {
+    const int b = (int)grp.basis_function_id;
+    if (!grp.h_radii || grp.number_of_terms <= 0 || (b != (int)SPH && b != (int)WENDLAND_D3_C2)) return nullptr;
+    if (!(gs.radius_min > 0.f) || !(gs.radius_max > gs.radius_min) || !std::isfinite(gs.radius_max)) return nullptr;
+    auto hs = std::make_shared<HBinStats>();
+    hs->h_min = gs.radius_min;
+    hs->h_max = gs.radius_max;
+    hs->edges = hbin_fine_edges(gs.radius_min, gs.radius_max);
+    hs->count.assign(kHBinFine, 0);
+    hs->wmax.assign(kHBinFine, 0.f);
+    for (int k = 0; k < grp.number_of_terms; ++k) {
+        const int f = hbin_fine_index(hs->edges, grp.h_radii[k]);
+        hs->count[f] += 1;
+        hs->wmax[f] = std::max(hs->wmax[f], std::fabs(grp.h_constraints[k].weight));
+    }
+    hs->id = g_hbin_ids.fetch_add(1) + 1;
+    return hs;
+}
+}  // namespace
+
 // ------------------------------------------------------ registration pool
 // Registered particle arrays come from a stream-ordered memory pool of the
 // library's own, one per device, that keeps freed blocks (release threshold
@@ -561,6 +609,7 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
                 gs.radius_min = std::min(gs.radius_min, grp.h_radii[k]);
                 gs.radius_max = std::max(gs.radius_max, grp.h_radii[k]);
             }
+            gs.hbins = hbin_histogram(grp, gs);
         }
         {
             std::lock_guard<std::mutex> lock(g_stats_mu);
@@ -758,6 +807,7 @@ SumRequest spectrum_request(const VisSpectrum* sp, const Group& grp, ConfigState
     r.radius_min = gs.radius_min;
     r.radius_max = gs.radius_max;
     r.weight_max = gs.weight_max;
+    r.hbins = gs.hbins.get();  // kept alive by the registration table until unregistered
     r.n = grp.number_of_terms;
     r.basis = (int)grp.basis_function_id;
     r.lat.x0 = -sp->grid.x / 2;
@@ -833,7 +883,7 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
             return set_error(kNotRegistered, "vis_spectrum_compute: group not registered");
         SumRequest r = spectrum_request(sp, grp, s);
         const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
-        if (want_tc && tensor_sum_available(r)) tc_groups.push_back(r);
+        if (want_tc && tensor_sum_available(r, form)) tc_groups.push_back(r);
         else plain_groups.push_back(r);
     }
     // every group adds into a zeroed spectrum (the result equals the
@@ -1046,7 +1096,7 @@ int batch_build(VisBatch* b, ConfigState* s, int form) {
                 return set_error(kNotRegistered, "vis_batch_execute: a group of a batch dataset is not registered");
             SumRequest r = spectrum_request(j.sp, grp, s);
             const bool want_tc = form == VIS_FORM_TENSOR || form == VIS_FORM_AUTO;
-            if (want_tc && tensor_sum_available(r)) b->tc_groups.push_back(r);
+            if (want_tc && tensor_sum_available(r, form)) b->tc_groups.push_back(r);
             else b->plain_groups.push_back(r);
         }
     int rc = kOk;

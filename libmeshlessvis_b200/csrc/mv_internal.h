@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -42,6 +43,24 @@ struct Lattice {
     double m[9];
 };
 
+// Smoothing-length histogram of a registered group whose transform does not
+// separate per axis (SPH, WENDLAND_D3_C2 with per-particle radii): kHBinFine
+// log-spaced fine bins between the smallest and the largest radius, with the
+// particle count and the largest |weight| of each.  Fine bin of radius h: the
+// largest i with edge[i] <= h, clamped to [0, kHBinFine); host and device
+// classify by the same float comparisons against the same edges, so counts
+// taken at registration hold for the device's scatter at compute time.
+constexpr int kHBinFine = 1024;
+struct HBinStats {
+    float h_min = 0.f, h_max = 0.f;
+    std::vector<float> edges;  // kHBinFine + 1
+    std::vector<int> count;    // kHBinFine
+    std::vector<float> wmax;   // kHBinFine
+    unsigned long long id = 0;  // unique per registration (cache key)
+};
+std::vector<float> hbin_fine_edges(float h_min, float h_max);
+int hbin_fine_index(const std::vector<float>& edges, float h);
+
 // One group's Fourier sum over a lattice, written to `out` as
 //   out[idx] (=|+=) scale * sum_j w_j Phi^(|k| h_j) exp(-2 pi i n.(M p_j))
 // where idx = out_base + (x-x0) out_sx + (y-y0) out_sy + (z-z0) out_sz
@@ -53,6 +72,7 @@ struct SumRequest {
     float radius_min;         // smallest / largest radius and largest |weight|
     float radius_max;         //   when known (registration), else < 0
     float weight_max;
+    const HBinStats* hbins;   // smoothing-length histogram (registration), or null
     int n;
     int basis;
     Lattice lat;
@@ -124,12 +144,13 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 //                         stream-ordered and capturable once the workspaces
 //                         are large enough.
 // The spectra must be zeroed (or hold earlier groups) before tensor_enqueue.
-int tensor_sum_available(const SumRequest& req);
+// form: VIS_FORM_TENSOR or VIS_FORM_AUTO (h-binned groups only when cheaper).
+int tensor_sum_available(const SumRequest& req, int form);
 
 // One job of the persistent tensor-core kernel: a separable group summed over
 // a lattice of rows (a, b) and columns c >= 0 into an FP64 accumulator.  Its
 // work items are (split ks, m tile, n tile), local index (ks * n_mtiles +
-// m_tile) * n_ntiles + n_tile.  Device-resident (88 bytes).
+// m_tile) * n_ntiles + n_tile.  Device-resident (104 bytes).
 //
 // Frequencies: a = a_idx + a_base, b = b_idx + b_base, c = c_idx + c_base.
 // A group's planes c < Kz/2 are one job (a_base = -Kx/2, b_base = -Ky/2,
@@ -163,9 +184,51 @@ struct TcJob {
     const unsigned char* bimg;  // B-operand images, or null
     int n_blocks;    // 32-particle blocks
     int img_stride;  // bytes per image: 512 x (c values per CTA of a full n-tile)
+    // h-binned jobs (period > 0): the job's lz_tc = P x period columns are P
+    // blocks of `period` frequency columns, block q weighted on the B side by
+    // the Chebyshev polynomial T_q(t_j) of the particle's normalised radius t_j
+    // in its bin (kept in the constants' gam field).  Each dumped value is
+    // multiplied by coef[q * coef_stride + a^2 + b^2 + c^2], the q-th Chebyshev
+    // coefficient of h -> Phi^(|k| h) over the bin, and added into the
+    // accumulator column c = column % period.
+    const float* coef;
+    int period;
+    int coef_stride;
+};
+
+// The h-bins of one binned group on one lattice (tensor_plan): consecutive
+// runs of fine bins, each with its Chebyshev order and weight scale.
+struct HBin {
+    int f0, f1;      // fine bins [f0, f1)
+    float lo, hi;    // radius interval (fine edges f0, f1)
+    int count;       // particles
+    float wmax;      // largest |weight|
+    int order;       // Chebyshev nodes P
+};
+struct HBinPlan {
+    std::vector<HBin> bins;
+    double cost = 0.0;      // sum over bins of count x order, per particle
+    bool feasible = true;   // false: some radii need more Chebyshev nodes than a bin may have
 };
 
 struct TensorPlan {
+    // A binned group's device tables, uploaded with the job table: bin edges
+    // (nbins + 1 floats), then per bin int4 (first block, count, coef offset,
+    // order) and float2 (2^12 / W, Chebyshev node scale), then the counters
+    // the scatter uses (in the accumulator workspace, zeroed per compute).
+    struct Binned {
+        int group;
+        int nbins;
+        size_t meta_offset;     // edges, then int4 bin table, then float2 bin scales
+        size_t cursor_offset;   // into acc (ints)
+        size_t coef_offset;     // into coef (floats)
+        size_t coef_count;
+        int nsq;                // coefficient table stride: max a^2 + b^2 + c^2 + 1
+        std::vector<HBin> bins;
+        std::vector<float> edges;  // nbins + 1: the fine edges where the bins start (classification)
+    };
+    std::vector<Binned> binned;
+    size_t coef_bytes = 0;
     struct Class {
         float2* out;
         int kx, ky, lz_tc, lz_out;
@@ -185,6 +248,12 @@ struct TensorPlan {
     std::vector<Class> classes;
     std::vector<int> group_class, job_of_group;
     std::vector<int> nyq_job_of_group;  // the transposed Nyquist-plane jobs (a >= 0 here, a < 0 next), or -1
+    std::vector<int> group_binned;      // index into binned, or -1
+    // per job: its particle constants (offset into the particles workspace),
+    // accumulator class and part (0 planes, 1 Nyquist a >= 0, 2 Nyquist a < 0),
+    // coefficient table (offset in floats into coef, SIZE_MAX for none)
+    std::vector<size_t> job_tp, job_coef;
+    std::vector<int> job_class, job_acc;
     std::vector<size_t> tp_offset, tp_nyq_offset;
     std::vector<size_t> bimg_offset;  // per job: its B-operand images in the workspace, or SIZE_MAX
     size_t bimg_bytes = 0;
@@ -200,6 +269,7 @@ struct TensorWorkspace {
     Workspace acc;        // FP64 accumulators
     Workspace meta;       // job and item tables
     Workspace bimg;       // B-operand images
+    Workspace coef;       // Chebyshev coefficient tables of h-binned groups
     std::vector<char> uploaded;  // the tables last copied to `meta`
     void* uploaded_to = nullptr;
     void release() {
@@ -209,6 +279,7 @@ struct TensorWorkspace {
         acc.release();
         meta.release();
         bimg.release();
+        coef.release();
     }
 };
 
@@ -236,6 +307,7 @@ struct TuneParams {
     int tc_waves = 4;     // tensor form: particle splits until the items make ~tc_waves waves
     int tc_flush = 16;    // tensor form, single-accumulator tiles: stages per TMEM chain (8 or 16;
                           // the double-buffered 128x128 tile uses at most 8)
+    int hbin_job_cost = 1024;  // h-binned groups: cost of one more bin (a job), in particle x node units
 };
 // The parameters in force on this thread: set by TuneScope around a compute.
 const TuneParams& active_tune();
@@ -251,6 +323,7 @@ TuneParams tuned_params(int kx, int ky, int kz, long long n_total, int n_groups,
 // and keyed by the group's device particle pointer; all -1 if unknown.
 struct GroupStats {
     float radius_min = -1.f, radius_max = -1.f, weight_max = -1.f;
+    std::shared_ptr<const HBinStats> hbins;  // SPH / Wendland groups with varying radii
 };
 GroupStats registered_group_stats(const void* d_constraints);
 

@@ -74,10 +74,15 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 
+#include "meshless_vis_b200.h"
 #include "mv_device.cuh"
 #include "mv_internal.h"
 
@@ -202,6 +207,7 @@ struct TcItem {
     int bc0, bnc;  // the c values whose B rows this CTA produces: all of them, or one half (kPair)
     int row0;      // this CTA's first lattice row
     int a_base, b_base, c_base;  // the job's frequency offsets, in registers for the stage loops
+    int period;                  // h-binned job: frequency columns per Chebyshev block (else 0)
     const unsigned char* bimg;   // this CTA's B-operand images of the item's n-tile (one per block), or null
     int img_stride, img_bytes;   // bytes between images; bytes of one image (512 bnc)
 };
@@ -228,6 +234,7 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.a_base = r.job->a_base;
     r.b_base = r.job->b_base;
     r.c_base = r.job->c_base;
+    r.period = r.job->period;
     r.img_stride = r.job->img_stride;
     r.img_bytes = 4 * r.bnc * kRowBytes;
     r.bimg = r.job->bimg ? r.job->bimg + (size_t)(r.n_tile * Shape<MODE>::kCtas + rank) * r.job->n_blocks *
@@ -526,15 +533,37 @@ __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int 
     }
 }
 
-// One B unit: c values c_s .. c_s + 7 (c_s >= 0; the chain rises) of a
-// particle pair (fixed-point z turns pqz, Gaussian exponents pgam; unit
-// rotations RX, RY, NRY = -RY and Gaussian ratios RHO as in rotate_pair), into
-// a B operand of bnc c values at bhi: rows chunk*8 .. +7 of its Re F half and
-// of its Im F half, hi rows then lo rows 2 bnc rows later.  The producer warps
-// run it into the stage buffer and tc_bimg_kernel into global memory: one
-// arithmetic for both.
-__device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col, int c_s, const uint32_t* pqz,
-                                       const float* pgam, bool gauss, float2 RX, float2 RY, float2 NRY, float2 RHO) {
+// Chebyshev polynomial T_q(t) by the three-term recurrence.
+__device__ __forceinline__ float chebyshev_t(int q, float t) {
+    float t0 = 1.f, t1 = t;
+    if (q == 0) return 1.f;
+    for (int i = 1; i < q; ++i) {
+        const float t2 = fmaf(2.f * t, t1, -t0);
+        t0 = t1;
+        t1 = t2;
+    }
+    return t1;
+}
+
+// One B unit: the job's columns c_col .. c_col + 7 of a particle pair
+// (fixed-point z turns pqz, Gaussian exponents pgam -- for h-binned jobs the
+// particles' normalised radii t in their bin; unit rotations RX, RY, NRY = -RY
+// and Gaussian ratios RHO as in rotate_pair), into a B operand of bnc c values
+// at bhi: rows chunk*8 .. +7 of its Re F half and of its Im F half, hi rows
+// then lo rows 2 bnc rows later.  Column c_col is frequency c_col + c_base; in
+// an h-binned job (period > 0) it is frequency c_col % period + c_base of
+// Chebyshev block q = c_col / period, weighted by T_q(t).  The chain's 8
+// frequencies c_s .. c_s + 7 rise from c_s >= 0 and never cross a block (the
+// period is a multiple of 8).  The producer warps run it into the stage
+// buffer and tc_bimg_kernel into global memory: one arithmetic for both.
+__device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col, int c_col, int c_base, int period,
+                                       const uint32_t* pqz, const float* pgam, bool gauss, float2 RX, float2 RY,
+                                       float2 NRY, float2 RHO) {
+    int c_s = c_col + c_base, cheb = -1;
+    if (period > 0) {
+        cheb = c_col / period;
+        c_s = c_col - cheb * period + c_base;
+    }
     float v[2][3];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -544,6 +573,8 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
         if (gauss) {
             g *= exp2f(pgam[e] * (float)(c_s * c_s));
             q = exp2f(pgam[e] * (float)(2 * c_s + 1));
+        } else if (cheb >= 0) {
+            g *= chebyshev_t(cheb, pgam[e]);
         }
         v[e][0] = g * cs;
         v[e][1] = -g * sn;
@@ -558,6 +589,30 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
     if (gauss) b_chain<true>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY,
                              make_float2(v[0][2], v[1][2]), RHO);
     else b_chain<false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, make_float2(1.f, 1.f), RHO);
+}
+
+// The dump of an h-binned job's 32 total columns cc .. cc + 31 for one row
+// (out of line: the Chebyshev bookkeeping stays out of the kernel's register
+// budget).  Column c is Chebyshev block q = c / period at frequency column
+// c % period; its value is weighted by the block's coefficient at |k|^2 =
+// a^2 + b^2 + c^2 and added into that frequency column of the accumulator.
+__device__ __noinline__ void dump_binned(const TcItem& I, const float* tt, int cc, int ncols, int half_cols, int rho,
+                                         bool in_rows, size_t mk, double* acc, double dump_scale) {
+    if (!in_rows) return;
+    const int a_f = rho / I.job->ky + I.a_base, b_f = rho % I.job->ky + I.b_base;
+    const int ab2 = a_f * a_f + b_f * b_f;
+    const float* coef = I.job->coef;
+    const int stride = I.job->coef_stride;
+    for (int i = 0; i < 32; ++i) {
+        const int n = cc + i;
+        if (n >= ncols) break;
+        const int h = n / half_cols, nn = n - h * half_cols;
+        const int im = nn >= I.bnc ? 1 : 0;
+        const int c = I.c0 + h * I.bnc + nn - im * I.bnc;
+        const int q = c / I.period, cf = c - q * I.period, cfreq = cf + I.c_base;
+        const double w = (double)__ldg(coef + (size_t)q * stride + ab2 + cfreq * cfreq);
+        atomicAdd(acc + (size_t)(2 * cf + im) * mk + rho, (double)tt[i] * dump_scale * w);
+    }
 }
 
 // Persistent: CTA (or CTA pair) b walks items b, b + grid, ... of the
@@ -763,7 +818,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     }
                     if (!dump) {
                         tmem_st32(lane_base + kColTotal + cc, tt);
-                    } else {
+                    } else if (I.period == 0) {
                         // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are
                         // contiguous.  Column n: CTA h = n / half_cols's B rows,
                         // Re then Im of its bnc c values.
@@ -777,6 +832,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                                 atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
                             }
                         }
+                    } else {
+                        dump_binned(I, tt, cc, ncols, half_cols, rho, in_rows, mk, acc, dump_scale);
                     }
                 }
                 tc_fence_before();
@@ -962,8 +1019,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.bnc || I.bimg) break;  // the loader copies B images
-                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8 + I.c_base, pqz, pgam, gauss, RX, RY, NRY,
-                               RHO);
+                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8, I.c_base, I.period, pqz, pgam, gauss, RX, RY,
+                               NRY, RHO);
                     }
                 }
                 // each thread makes its stores visible to the tensor core; the
@@ -1070,6 +1127,122 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
     }
 }
 
+// h-bins of a group whose Phi^ does not separate per axis (SPH, Wendland with
+// per-particle radii).  Within bin b (radii in [lo, hi]) Phi^(|k| h) is
+// replaced by its Chebyshev interpolant in h on the bin's `order` Chebyshev
+// nodes h_p:
+//   Phi^(|k| h_j) ~= sum_q c_q(|k|) T_q(t_j),  t_j = (2 h_j - lo - hi) / (hi - lo),
+//   c_q(|k|) = (2 / P) sum_p Phi^(|k| h_p) T_q(x_p)  (c_0 halved),
+// so the bin's sum is, per q, a separable sum with B-side weights T_q(t_j)
+// (one job per bin whose columns are the q blocks), and c_q(|k|) multiplies
+// the q-th block when it is dumped.  The bins and orders are chosen on the
+// host (hbin_plan) so the interpolation error stays near 1e-6 of the sum.
+
+// Bin of radius h among nb bins with edges e[0..nb]: the largest i with
+// e[i] <= h, clamped to [0, nb) -- the rule hbin_fine_index applies to the
+// fine edges at registration, whose counts the bins' capacities come from.
+__device__ __forceinline__ int hbin_of(const float* e, int nb, float h) {
+    if (nb <= 1 || !(h >= e[1])) return 0;
+    if (h >= e[nb - 1]) return nb - 1;
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (e[mid] <= h) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+struct TcBinnedPrepArgs {
+    const float4* particles;
+    const float* radii;
+    int n;
+    double step;
+    int nbins;
+    const float* edges;    // nbins + 1 classification edges
+    const int4* bins;      // (first block, capacity, coef offset, order)
+    const float4* spans;   // (lo, hi, 2^12 / W_b, 0): Chebyshev interval and weight scale
+    int* cursors;          // nbins, zero at launch
+    uint8_t* out;          // the group's blocks, bin by bin
+    uint8_t* out_nyq;      // the same with x and z exchanged, or null
+    int* error_flag;
+};
+
+// Scatters each particle's constants into its bin's blocks (order within a
+// bin follows the atomic counter); gam holds t, the normalised radius.  The
+// blocks were zeroed first, so padding particles have zero amplitude.
+__global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= p.n) return;
+    const float h = p.radii[j];
+    const int b = hbin_of(p.edges, p.nbins, h);
+    const int4 bin = p.bins[b];
+    const int slot = atomicAdd(p.cursors + b, 1);
+    if (slot >= bin.y) {  // the registered histogram does not hold for these radii
+        atomicOr(p.error_flag, 2048);
+        return;
+    }
+    const float4 sp = p.spans[b];
+    const float t = sp.y > sp.x ? (2.f * h - sp.x - sp.y) / (sp.y - sp.x) : 0.f;
+    const float4 q = p.particles[j];
+    const uint32_t qx = fixed_turns(p.step * (double)q.x);
+    const uint32_t qy = fixed_turns(p.step * (double)q.y);
+    const uint32_t qz = fixed_turns(p.step * (double)q.z);
+    const float amp = q.w * sp.z;
+    const size_t blk_off = (size_t)(bin.x + slot / kBlockParticles) * kBlockBytes;
+    const int l = slot % kBlockParticles;
+    const float2 ry = unit_phase(qy);
+    for (int pass = 0; pass < (p.out_nyq ? 2 : 1); ++pass) {
+        uint8_t* blk = (pass == 0 ? p.out : p.out_nyq) + blk_off;
+        const uint32_t ax = pass == 0 ? qx : qz, az = pass == 0 ? qz : qx;
+        reinterpret_cast<uint32_t*>(blk + kOffQx)[l] = ax;
+        reinterpret_cast<uint32_t*>(blk + kOffQy)[l] = qy;
+        reinterpret_cast<uint32_t*>(blk + kOffQz)[l] = az;
+        reinterpret_cast<float*>(blk + kOffAmp)[l] = amp;
+        reinterpret_cast<float*>(blk + kOffGam)[l] = t;
+        reinterpret_cast<float*>(blk + kOffRho2)[l] = 1.f;
+        reinterpret_cast<float2*>(blk + kOffRy)[l] = ry;
+        reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(az);
+    }
+}
+
+struct TcCoefArgs {
+    int basis;
+    double step;
+    int nbins;
+    int nsq;               // entries per (bin, q): |k|^2 / step^2 = 0 .. nsq - 1
+    const int4* bins;      // (first block, capacity, coef offset, order)
+    const float4* spans;   // (lo, hi, ...)
+    float* coef;
+};
+
+// Chebyshev coefficients c_q(|k|) of h -> Phi^(|k| h) on each bin, for every
+// integer |k|^2 / step^2 of the lattice, in FP64 (the reference's Phi^
+// formulas), stored as floats: coef[offset + q * nsq + n2].
+__global__ void tc_coef_kernel(TcCoefArgs c) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)c.nbins * c.nsq) return;
+    const int b = (int)(i / c.nsq), n2 = (int)(i % c.nsq);
+    const int4 bin = c.bins[b];
+    const float4 sp = c.spans[b];
+    const int order = bin.w;
+    const double k = c.step * sqrt((double)n2);
+    const double mid = 0.5 * ((double)sp.x + (double)sp.y), half = 0.5 * ((double)sp.y - (double)sp.x);
+    constexpr int kMaxOrder = 16;
+    double f[kMaxOrder], x[kMaxOrder];
+    for (int p = 0; p < order && p < kMaxOrder; ++p) {
+        x[p] = cospi((2.0 * p + 1.0) / (2.0 * order));
+        f[p] = phi_fp64(c.basis, k * (mid + half * x[p]));
+    }
+    for (int q = 0; q < order && q < kMaxOrder; ++q) {
+        double acc = 0.0;
+        for (int p = 0; p < order; ++p) acc += f[p] * cospi(q * (2.0 * p + 1.0) / (2.0 * order));
+        acc *= 2.0 / order;
+        if (q == 0) acc *= 0.5;
+        c.coef[(size_t)bin.z + (size_t)q * c.nsq + n2] = (float)acc;
+    }
+}
+
 // B-operand images of one job (layout in TcJob): one CTA per image (n-tile,
 // CTA half, 32-particle block); thread (chunk, pair) runs b_unit for 8 c
 // values of 2 particles, exactly as a producer warp would into the stage
@@ -1079,7 +1252,7 @@ struct TcImageArgs {
     const unsigned char* blocks;
     unsigned char* bimg;
     int n_blocks, img_stride;
-    int ctas, nc_tile, lz_tc, c_base;
+    int ctas, nc_tile, lz_tc, c_base, period;
     bool gauss;
 };
 
@@ -1103,7 +1276,8 @@ __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
     const float2 NRY = make_float2(-RY.x, -RY.y);
     const float2 RHO = g.gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
     uint8_t* out = g.bimg + (size_t)img * g.img_stride;
-    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8 + g.c_base, pqz, pgam, g.gauss, RX, RY, NRY, RHO);
+    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, g.c_base, g.period, pqz, pgam, g.gauss, RX, RY, NRY,
+           RHO);
 }
 
 // acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
@@ -1248,7 +1422,139 @@ extern "C" void vis_set_operand_cache_limit(long long bytes) {
     __atomic_store_n(&g_operand_cache_limit, bytes < 0 ? -1LL : bytes, __ATOMIC_RELAXED);
 }
 
-int tensor_sum_available(const SumRequest& r) {
+namespace {
+
+// ---------------------------------------------------------------- h-bins
+// Chebyshev order of a bin whose radii span dh at the lattice's largest |k|:
+// the smallest P with 2 (pi x / 4)^P / P! <= kHBinTau, x = |k|max dh (the
+// interpolation error bound of an oscillation of that frequency, with the
+// constant set on the sums' FP64 error: about 1e-6 rel-L2 on SPH and Wendland
+// sets with 58x ranges of h); bins needing more than kHBinMaxOrder nodes are
+// not formed.
+constexpr double kHBinTau = 3e-6;
+constexpr int kHBinMaxOrder = 12;
+
+double hbin_order_limit(int order) {  // largest x that `order` nodes cover
+    double f = 1.0;
+    for (int i = 2; i <= order; ++i) f *= i;
+    return (4.0 / kPi) * std::pow(kHBinTau * f / 2.0, 1.0 / order);
+}
+
+int hbin_order(double x) {
+    static const std::vector<double> limit = [] {
+        std::vector<double> v(kHBinMaxOrder + 1, 0.0);
+        for (int p = 1; p <= kHBinMaxOrder; ++p) v[p] = hbin_order_limit(p);
+        return v;
+    }();
+    for (int p = 1; p <= kHBinMaxOrder; ++p)
+        if (x <= limit[p]) return p;
+    return kHBinMaxOrder + 1;
+}
+
+// The largest |k| of a half-spectrum lattice and the largest a^2 + b^2 + c^2.
+long long lattice_nsq(const Lattice& L) {
+    const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz - 1;
+    return hx * hx + hy * hy + hz * hz;
+}
+
+// Bins of a group on a lattice: runs of fine bins chosen by dynamic
+// programming to minimise sum(count x order) + job_cost per non-empty bin
+// (a bin is one more job: its items, pipeline fills and accumulator dumps),
+// each bin's Chebyshev interval the span of its non-empty fine bins.
+HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int job_cost) {
+    const int F = kHBinFine;
+    std::vector<long long> cum(F + 1, 0);
+    for (int f = 0; f < F; ++f) cum[f + 1] = cum[f] + hs.count[f];
+    std::vector<int> first_ne(F + 1, F), last_ne(F + 1, -1);  // first non-empty >= i, last non-empty < j
+    for (int f = F - 1; f >= 0; --f) first_ne[f] = hs.count[f] ? f : first_ne[f + 1];
+    for (int f = 0; f < F; ++f) last_ne[f + 1] = hs.count[f] ? f : last_ne[f];
+    std::vector<double> best(F + 1, 1e300);
+    std::vector<int> arg(F + 1, 0);
+    best[0] = 0.0;
+    for (int j = 1; j <= F; ++j) {
+        for (int i = j - 1; i >= 0; --i) {
+            const long long n = cum[j] - cum[i];
+            int order = 1;
+            if (n > 0) {
+                const double dh = (double)hs.edges[last_ne[j] + 1] - (double)hs.edges[first_ne[i]];
+                order = hbin_order(kmax * dh);
+                if (order > kHBinMaxOrder) break;  // wider runs only need more
+            }
+            const double c = best[i] + (double)n * order + (n > 0 ? job_cost : 0);
+            if (c < best[j]) {
+                best[j] = c;
+                arg[j] = i;
+            }
+        }
+    }
+    HBinPlan plan;
+    if (!(best[F] < 1e299)) {  // a single fine bin already needs too many nodes
+        plan.feasible = false;
+        return plan;
+    }
+    std::vector<int> cuts;
+    for (int j = F; j > 0; j = arg[j]) cuts.push_back(j);
+    cuts.push_back(0);
+    std::reverse(cuts.begin(), cuts.end());
+    long long total = 0, weighted = 0;
+    for (size_t k = 0; k + 1 < cuts.size(); ++k) {
+        HBin b;
+        b.f0 = cuts[k];
+        b.f1 = cuts[k + 1];
+        b.count = (int)(cum[b.f1] - cum[b.f0]);
+        b.wmax = 0.f;
+        for (int f = b.f0; f < b.f1; ++f) b.wmax = std::max(b.wmax, hs.wmax[f]);
+        if (b.count > 0) {
+            b.lo = hs.edges[first_ne[b.f0]];
+            b.hi = hs.edges[last_ne[b.f1] + 1];
+            b.order = hbin_order(kmax * ((double)b.hi - (double)b.lo));
+        } else {
+            b.lo = hs.edges[b.f0];
+            b.hi = hs.edges[b.f1];
+            b.order = 1;
+        }
+        total += b.count;
+        weighted += (long long)b.count * b.order;
+        plan.bins.push_back(b);
+    }
+    plan.cost = total > 0 ? (double)weighted / (double)total : 0.0;
+    return plan;
+}
+
+// Plans are cached per registration, lattice and job cost.
+std::mutex g_hbin_mu;
+std::map<std::tuple<unsigned long long, long long, double, int>, std::shared_ptr<const HBinPlan>> g_hbin_cache;
+
+std::shared_ptr<const HBinPlan> hbin_plan(const SumRequest& r) {
+    const long long nsq = lattice_nsq(r.lat);
+    const double kmax = r.lat.kx * std::sqrt((double)nsq);
+    const int job_cost = std::max(0, active_tune().hbin_job_cost);
+    const auto key = std::make_tuple(r.hbins->id, nsq, r.lat.kx, job_cost);
+    std::lock_guard<std::mutex> lock(g_hbin_mu);
+    auto it = g_hbin_cache.find(key);
+    if (it != g_hbin_cache.end()) return it->second;
+    if (g_hbin_cache.size() >= 256) g_hbin_cache.clear();
+    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, job_cost));
+    g_hbin_cache[key] = plan;
+    return plan;
+}
+
+// A group the tensor form takes through h-bins: SPH or Wendland with varying
+// radii and a registered histogram.
+bool binned_group(const SumRequest& r) {
+    const bool uniform = r.radii && r.radius_min >= 0.f && r.radius_min == r.radius_max;
+    return r.radii && !uniform && (r.basis == kSph || r.basis == kWendland) && r.hbins &&
+           (int)r.hbins->count.size() == kHBinFine;
+}
+
+// The automatic choice takes the h-binned tensor form while its work (terms x
+// mean Chebyshev order) stays below what the plain form costs, which does
+// about a tenth of the tensor form's terms per second.
+constexpr double kHBinAutoMaxCost = 6.0;
+
+}  // namespace
+
+int tensor_sum_available(const SumRequest& r, int form) {
     const Lattice& L = r.lat;
     if (!is_spectrum_lattice(L) || r.wrap != 0) return 0;
     const int lz_tc = L.nz - 1;  // planes [0, Kz/2); the Nyquist plane is planned separately
@@ -1257,21 +1563,28 @@ int tensor_sum_available(const SumRequest& r) {
     if (r.weight_max < 0.f) return 0;  // needs the registered |weight| maximum
     const bool uniform = r.radii && r.radius_min >= 0.f && r.radius_min == r.radius_max;
     const bool separable = !r.radii || uniform || r.basis == kGaussianDecaying;
-    return separable ? 1 : 0;
+    if (separable) return 1;
+    if (!binned_group(r)) return 0;
+    if ((long long)L.nx * L.ny * lz_tc * 2 * kHBinMaxOrder > (1LL << 31)) return 0;
+    const std::shared_ptr<const HBinPlan> hp = hbin_plan(r);
+    if (!hp->feasible) return 0;
+    if (form == VIS_FORM_TENSOR) return 1;
+    return hp->cost <= kHBinAutoMaxCost ? 1 : 0;
 }
 
 namespace {
 
 // Groups that can share an FP64 accumulator: same output spectrum and the
-// same per-frequency factor (none for Gaussian jobs; Phi^(|k| h) with the
-// same basis and h for factored ones).
+// same per-frequency factor (none for Gaussian and h-binned jobs, whose
+// factors are applied per particle or per dump; Phi^(|k| h) with the same
+// basis and h for factored ones).
 struct ClassKey {
     const float2* out;
-    int gauss;
+    int unfactored;
     int basis;
     double h;
     bool operator==(const ClassKey& o) const {
-        return out == o.out && gauss == o.gauss && (gauss || (basis == o.basis && h == o.h));
+        return out == o.out && unfactored == o.unfactored && (unfactored || (basis == o.basis && h == o.h));
     }
 };
 
@@ -1294,7 +1607,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     // items appended, B-operand images where the job allows them (image_ok)
     // and they fit the limit; returns the job's index.
     const size_t image_limit = operand_cache_limit();
-    auto add_job = [&](TcJob j, int mode, bool image_ok) {
+    auto add_job = [&](TcJob j, int mode, bool image_ok, size_t tp_offset, int cls, int acc_part,
+                       size_t coef_offset) {
         // equal n-tiles of at most kNc c values: 192 planes -> 96 + 96 (two
         // N = 192 MMAs) rather than 128 + 64 (an N = 128 one, bound by its
         // shared-memory operand reads); multiples of 16 for kPair
@@ -1328,6 +1642,10 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         const int job_index = (int)plan.jobs.size();
         plan.jobs.push_back(j);
         plan.bimg_offset.push_back(img_off);
+        plan.job_tp.push_back(tp_offset);
+        plan.job_class.push_back(cls);
+        plan.job_acc.push_back(acc_part);
+        plan.job_coef.push_back(coef_offset);
         const int flush = narrow_mode(mode) ? plan.flush_narrow : plan.flush;
         for (long long ks = 0; ks < splits; ++ks) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
@@ -1337,13 +1655,21 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         }
         return job_index;
     };
+    // tile mode of a job with `cols` columns over kx * ky rows: kNarrow up to
+    // 64 columns; beyond, kPair where every n-tile splits into two halves of
+    // 8-c chunks and the rows into 256-row m-tiles, else kWide
+    auto mode_of = [](int cols, long long rows) {
+        const bool pairs = tc_pairs_enabled() && cols % 16 == 0 && rows % 256 == 0;
+        return cols <= Shape<kNarrow>::kNc ? (pairs ? kPairNarrow : kNarrow) : (pairs ? kPair : kWide);
+    };
     for (size_t g = 0; g < groups.size(); ++g) {
         const SumRequest& r = groups[g];
         const Lattice& L = r.lat;
         const int kx = L.nx, ky = L.ny, lz_out = L.nz, lz_tc = L.nz - 1;
         const bool uniform = r.radii && r.radius_min >= 0.f && r.radius_min == r.radius_max;
         const bool gauss = r.radii && !uniform && r.basis == kGaussianDecaying;
-        ClassKey key{r.out, gauss ? 1 : 0, r.basis, uniform ? (double)r.radius_max : 1.0};
+        const bool binned = !gauss && binned_group(r);
+        ClassKey key{r.out, (gauss || binned) ? 1 : 0, r.basis, uniform ? (double)r.radius_max : 1.0};
         int cls = -1;
         for (size_t c = 0; c < keys.size(); ++c)
             if (keys[c] == key) cls = (int)c;
@@ -1359,7 +1685,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             c.step = L.kx;
             c.basis = r.basis;
             c.h = key.h;
-            c.factored = !gauss;
+            c.factored = !key.unfactored;
             c.scale = r.scale;
             c.acc_offset = plan.acc_bytes;
             plan.acc_bytes += ((size_t)kx * ky * lz_tc * 2 * sizeof(double) + 255) / 256 * 256;
@@ -1368,21 +1694,110 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             plan.classes.push_back(c);
         }
         plan.group_class.push_back(cls);
-        const size_t blocks_bytes =
-            (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
-        plan.tp_offset.push_back(plan.tp_bytes);
-        plan.tp_bytes += blocks_bytes;
-        plan.tp_nyq_offset.push_back(0);
+        plan.group_binned.push_back(-1);
         plan.nyq_job_of_group.push_back(-1);
+        plan.tp_nyq_offset.push_back(0);
+        plan.tp_offset.push_back(plan.tp_bytes);
         if (r.n <= 0 || !(r.weight_max > 0.f)) {
             plan.job_of_group.push_back(-1);
             continue;
         }
-        // tile mode: kNarrow up to 64 tensor planes; beyond, kPair where every
-        // n-tile splits into two halves of 8-c chunks and the rows into
-        // 256-row m-tiles, else kWide
-        const bool pairs = tc_pairs_enabled() && lz_tc % 16 == 0 && ((long long)kx * ky) % 256 == 0;
-        const int mode = lz_tc <= Shape<kNarrow>::kNc ? (pairs ? kPairNarrow : kNarrow) : (pairs ? kPair : kWide);
+        const bool nyq_ok = ky % 16 == 0 && kx % 2 == 0 && (kx / 2) % 8 == 0;
+        // the Nyquist plane's accumulator, once per class
+        auto class_nyquist = [&]() {
+            TensorPlan::Class& c = plan.classes[cls];
+            if (!c.nyquist) {
+                c.nyquist = true;
+                c.acc_nyq_offset = plan.acc_bytes;
+                plan.acc_bytes += ((size_t)kx * ky * 2 * sizeof(double) + 255) / 256 * 256;
+            }
+        };
+        if (binned) {
+            // ------------------------------------------ h-binned group
+            const std::shared_ptr<const HBinPlan> hp = hbin_plan(r);
+            TensorPlan::Binned bg;
+            bg.group = (int)g;
+            bg.bins = hp->bins;
+            bg.nbins = (int)hp->bins.size();
+            for (const HBin& b : bg.bins) bg.edges.push_back(r.hbins->edges[b.f0]);
+            bg.edges.push_back(r.hbins->edges[kHBinFine]);
+            bg.nsq = (int)(lattice_nsq(L) + 1);
+            bg.meta_offset = 0;  // placed by tensor_reserve_upload
+            bg.cursor_offset = plan.acc_bytes;
+            plan.acc_bytes += ((size_t)bg.nbins * sizeof(int) + 255) / 256 * 256;
+            bg.coef_offset = plan.coef_bytes / sizeof(float);
+            size_t coef_count = 0;
+            std::vector<int> first_block(bg.nbins);
+            long long blocks = 0;
+            for (int b = 0; b < bg.nbins; ++b) {
+                first_block[b] = (int)blocks;
+                blocks += (bg.bins[b].count + kBlockParticles - 1) / kBlockParticles;
+                coef_count += (size_t)bg.bins[b].order * bg.nsq;
+            }
+            bg.coef_count = coef_count;
+            plan.coef_bytes += (coef_count * sizeof(float) + 255) / 256 * 256;
+            const size_t blocks_bytes = (size_t)blocks * kBlockBytes;
+            plan.tp_bytes += blocks_bytes;
+            // the Nyquist plane as transposed jobs needs whole 8-c blocks of
+            // Kx/2 columns (and 16 for pairs, per job below)
+            const bool nyq = nyq_ok;
+            if (nyq) {
+                plan.tp_nyq_offset.back() = plan.tp_bytes;
+                plan.tp_bytes += blocks_bytes;
+                class_nyquist();
+            }
+            size_t coef_at = 0;
+            int first_job = -1, first_nyq = -1;
+            for (int b = 0; b < bg.nbins; ++b) {
+                const HBin& bin = bg.bins[b];
+                const size_t coef_off = bg.coef_offset + coef_at;
+                coef_at += (size_t)bin.order * bg.nsq;
+                if (bin.count <= 0 || !(bin.wmax > 0.f)) continue;
+                TcJob j{};
+                j.kx = kx;
+                j.ky = ky;
+                j.lz_tc = bin.order * lz_tc;
+                j.a_base = -kx / 2;
+                j.b_base = -ky / 2;
+                j.c_base = 0;
+                j.n = bin.count;
+                j.gauss = 0;
+                j.wmax = bin.wmax;
+                j.period = lz_tc;
+                j.coef_stride = bg.nsq;
+                const size_t tp = plan.tp_offset.back() + (size_t)first_block[b] * kBlockBytes;
+                const int jm = add_job(j, mode_of(j.lz_tc, (long long)kx * ky), true, tp, cls, 0, coef_off);
+                if (first_job < 0) first_job = jm;
+                if (nyq) {
+                    TcJob t = j;
+                    t.kx = 1;
+                    t.ky = ky;
+                    t.lz_tc = bin.order * (kx / 2);
+                    t.period = kx / 2;
+                    t.a_base = lz_tc;
+                    t.b_base = -ky / 2;
+                    t.c_base = 0;
+                    const int nmode = mode_of(t.lz_tc, ky);
+                    const size_t tpn = plan.tp_nyq_offset.back() + (size_t)first_block[b] * kBlockBytes;
+                    const int jn = add_job(t, nmode, false, tpn, cls, 1, coef_off);
+                    if (first_nyq < 0) first_nyq = jn;
+                    t.a_base = -lz_tc;
+                    t.b_base = 1 - ky / 2;
+                    t.c_base = 1;
+                    add_job(t, nmode, false, tpn, cls, 2, coef_off);
+                }
+            }
+            plan.job_of_group.push_back(first_job);
+            plan.nyq_job_of_group.back() = nyq ? first_nyq : -1;
+            plan.group_binned.back() = (int)plan.binned.size();
+            plan.binned.push_back(std::move(bg));
+            continue;
+        }
+        // ------------------------------------------------ separable group
+        const size_t blocks_bytes =
+            (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
+        plan.tp_bytes += blocks_bytes;
+        const int mode = mode_of(lz_tc, (long long)kx * ky);
         TcJob j{};
         j.kx = kx;
         j.ky = ky;
@@ -1393,13 +1808,15 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
-        plan.job_of_group.push_back(add_job(j, mode, true));
+        plan.job_of_group.push_back(add_job(j, mode, true, plan.tp_offset.back(), cls, 0, SIZE_MAX));
         // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
         // -a > 0; see TcJob) in the same launch, where the Kx / 2 columns of
         // each split into whole n-tile units (16 c for kPair, else 8);
         // otherwise the plain form sums it.  Their Ky rows (8-row chunks of one
         // sign of b) need not fill the last m-tile.
-        if (ky % 16 == 0 && (kx / 2) % (pair_mode(mode) ? 16 : 8) == 0 && kx % 2 == 0) {
+        if (nyq_ok && (kx / 2) % (pair_mode(mode) ? 16 : 8) == 0) {
+            plan.tp_nyq_offset.back() = plan.tp_bytes;
+            plan.tp_bytes += blocks_bytes;
             TcJob t = j;
             t.kx = 1;
             t.ky = ky;
@@ -1407,19 +1824,13 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             t.a_base = lz_tc;
             t.b_base = -ky / 2;
             t.c_base = 0;
-            plan.nyq_job_of_group.back() = add_job(t, mode, false);  // one m-tile: no reuse
+            const size_t tpn = plan.tp_nyq_offset.back();
+            plan.nyq_job_of_group.back() = add_job(t, mode, false, tpn, cls, 1, SIZE_MAX);  // one m-tile: no reuse
             t.a_base = -lz_tc;
             t.b_base = 1 - ky / 2;
             t.c_base = 1;
-            add_job(t, mode, false);
-            plan.tp_nyq_offset.back() = plan.tp_bytes;
-            plan.tp_bytes += blocks_bytes;
-            TensorPlan::Class& c = plan.classes[cls];
-            if (!c.nyquist) {
-                c.nyquist = true;
-                c.acc_nyq_offset = plan.acc_bytes;
-                plan.acc_bytes += ((size_t)kx * ky * 2 * sizeof(double) + 255) / 256 * 256;
-            }
+            add_job(t, mode, false, tpn, cls, 2, SIZE_MAX);
+            class_nyquist();
         }
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
@@ -1436,7 +1847,15 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         plan.n_pair_narrow += it.mode == kPairNarrow ? 1 : 0;
         plan.n_pair += it.mode == kPair ? 1 : 0;
     }
-    plan.meta_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256 + plan.items.size() * sizeof(int2);
+    const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
+    plan.meta_bytes = jobs_bytes + ((plan.items.size() * sizeof(int2) + 255) / 256) * 256;
+    // the binned groups' tables: edges, int4 bins, float4 spans (16-byte aligned)
+    for (TensorPlan::Binned& bg : plan.binned) {
+        bg.meta_offset = plan.meta_bytes;
+        const size_t edges = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
+        plan.meta_bytes += edges + (size_t)bg.nbins * (sizeof(int4) + sizeof(float4));
+        plan.meta_bytes = (plan.meta_bytes + 255) / 256 * 256;
+    }
     return kOk;
 }
 
@@ -1445,33 +1864,45 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     if (st == kOk) st = ws.acc.reserve(std::max<size_t>(plan.acc_bytes, 256));
     if (st == kOk) st = ws.meta.reserve(std::max<size_t>(plan.meta_bytes, 256));
     if (st == kOk && plan.bimg_bytes) st = ws.bimg.reserve(plan.bimg_bytes);
+    if (st == kOk && plan.coef_bytes) st = ws.coef.reserve(plan.coef_bytes);
     if (st != kOk) return st;
-    for (size_t j = 0; j < plan.jobs.size(); ++j)
-        plan.jobs[j].bimg = plan.bimg_offset[j] == SIZE_MAX
-                                ? nullptr
-                                : static_cast<const unsigned char*>(ws.bimg.ptr) + plan.bimg_offset[j];
     char* tp_base = static_cast<char*>(ws.particles.ptr);
     char* acc_base = static_cast<char*>(ws.acc.ptr);
-    for (size_t g = 0; g < plan.job_of_group.size(); ++g) {
-        const int j = plan.job_of_group[g];
-        if (j < 0) continue;
-        const TensorPlan::Class& c = plan.classes[plan.group_class[g]];
-        plan.jobs[j].blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.tp_offset[g]);
-        plan.jobs[j].acc = reinterpret_cast<double*>(acc_base + c.acc_offset);
-        const int t = plan.nyq_job_of_group[g];
-        if (t < 0) continue;
-        // both Nyquist jobs read the same transposed constants; the a < 0
-        // job's Kx/2 columns come first in the accumulator, then the a >= 0 job's
+    for (size_t j = 0; j < plan.jobs.size(); ++j) {
+        TcJob& job = plan.jobs[j];
+        job.bimg = plan.bimg_offset[j] == SIZE_MAX ? nullptr
+                                                   : static_cast<const unsigned char*>(ws.bimg.ptr) + plan.bimg_offset[j];
+        job.blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.job_tp[j]);
+        const TensorPlan::Class& c = plan.classes[plan.job_class[j]];
+        // Nyquist jobs: the a < 0 job's Kx/2 columns come first in the
+        // accumulator, then the a >= 0 job's
         double* nyq_acc = reinterpret_cast<double*>(acc_base + c.acc_nyq_offset);
-        plan.jobs[t].blocks = plan.jobs[t + 1].blocks =
-            reinterpret_cast<const unsigned char*>(tp_base + plan.tp_nyq_offset[g]);
-        plan.jobs[t].acc = nyq_acc + (size_t)(c.kx / 2) * 2 * c.ky;
-        plan.jobs[t + 1].acc = nyq_acc;
+        job.acc = plan.job_acc[j] == 0   ? reinterpret_cast<double*>(acc_base + c.acc_offset)
+                  : plan.job_acc[j] == 1 ? nyq_acc + (size_t)(c.kx / 2) * 2 * c.ky
+                                         : nyq_acc;
+        job.coef = plan.job_coef[j] == SIZE_MAX ? nullptr : static_cast<const float*>(ws.coef.ptr) + plan.job_coef[j];
     }
     std::vector<char> meta(plan.meta_bytes, 0);
     const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
     if (!plan.jobs.empty()) std::memcpy(meta.data(), plan.jobs.data(), plan.jobs.size() * sizeof(TcJob));
     if (!plan.items.empty()) std::memcpy(meta.data() + jobs_bytes, plan.items.data(), plan.items.size() * sizeof(int2));
+    for (const TensorPlan::Binned& bg : plan.binned) {
+        float* edges = reinterpret_cast<float*>(meta.data() + bg.meta_offset);
+        const size_t edges_bytes = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
+        int4* bins = reinterpret_cast<int4*>(meta.data() + bg.meta_offset + edges_bytes);
+        float4* spans = reinterpret_cast<float4*>(bins + bg.nbins);
+        int block = 0;
+        size_t coef_at = bg.coef_offset;
+        for (int b = 0; b < bg.nbins; ++b) {
+            const HBin& bin = bg.bins[b];
+            edges[b] = bg.edges[b];
+            bins[b] = make_int4(block, bin.count, (int)coef_at, bin.order);
+            spans[b] = make_float4(bin.lo, bin.hi, bin.wmax > 0.f ? kOperandScale / bin.wmax : 0.f, 0.f);
+            block += (bin.count + kBlockParticles - 1) / kBlockParticles;
+            coef_at += (size_t)bin.order * bg.nsq;
+        }
+        edges[bg.nbins] = bg.edges[bg.nbins];
+    }
     plan.d_jobs = static_cast<const void*>(ws.meta.ptr);
     plan.d_items = static_cast<const void*>(static_cast<char*>(ws.meta.ptr) + jobs_bytes);
     if (meta.empty()) return kOk;
@@ -1540,6 +1971,49 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         const int j = plan.job_of_group[g];
         if (j < 0) continue;
         const SumRequest& r = groups[g];
+        if (plan.group_binned[g] >= 0) {
+            // h-binned: zeroed blocks (padding particles get zero amplitude),
+            // the scatter into the bins, and the bins' coefficient tables
+            const TensorPlan::Binned& bg = plan.binned[plan.group_binned[g]];
+            size_t blocks = 0;
+            for (const HBin& b : bg.bins) blocks += (size_t)((b.count + kBlockParticles - 1) / kBlockParticles);
+            char* tp = static_cast<char*>(ws.particles.ptr) + plan.tp_offset[g];
+            char* tpn = plan.nyq_job_of_group[g] >= 0 ? static_cast<char*>(ws.particles.ptr) + plan.tp_nyq_offset[g]
+                                                      : nullptr;
+            st = check_cuda(cudaMemsetAsync(tp, 0, blocks * kBlockBytes, stream), "cudaMemsetAsync(binned blocks)");
+            if (st == kOk && tpn)
+                st = check_cuda(cudaMemsetAsync(tpn, 0, blocks * kBlockBytes, stream), "cudaMemsetAsync(binned blocks)");
+            if (st != kOk) return st;
+            const char* meta = static_cast<const char*>(ws.meta.ptr) + bg.meta_offset;
+            const size_t edges_bytes = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
+            TcBinnedPrepArgs bp;
+            bp.particles = r.particles;
+            bp.radii = r.radii;
+            bp.n = r.n;
+            bp.step = r.lat.kx;
+            bp.nbins = bg.nbins;
+            bp.edges = reinterpret_cast<const float*>(meta);
+            bp.bins = reinterpret_cast<const int4*>(meta + edges_bytes);
+            bp.spans = reinterpret_cast<const float4*>(bp.bins + bg.nbins);
+            bp.cursors = reinterpret_cast<int*>(static_cast<char*>(ws.acc.ptr) + bg.cursor_offset);
+            bp.out = reinterpret_cast<uint8_t*>(tp);
+            bp.out_nyq = reinterpret_cast<uint8_t*>(tpn);
+            bp.error_flag = error_flag;
+            tc_prep_binned_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(bp);
+            count_launch();
+            TcCoefArgs ca;
+            ca.basis = r.basis;
+            ca.step = r.lat.kx;
+            ca.nbins = bg.nbins;
+            ca.nsq = bg.nsq;
+            ca.bins = bp.bins;
+            ca.spans = bp.spans;
+            ca.coef = static_cast<float*>(ws.coef.ptr);
+            const long long entries = (long long)bg.nbins * bg.nsq;
+            tc_coef_kernel<<<(unsigned)((entries + 127) / 128), 128, 0, stream>>>(ca);
+            count_launch();
+            continue;
+        }
         const Lattice& L = r.lat;
         TcPrepArgs pa;
         pa.particles = r.particles;
@@ -1569,6 +2043,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         ia.nc_tile = j.nc_tile;
         ia.lz_tc = j.lz_tc;
         ia.c_base = j.c_base;
+        ia.period = j.period;
         ia.gauss = j.gauss != 0;
         const long long images = (long long)j.n_ntiles * ia.ctas * j.n_blocks;
         tc_bimg_kernel<<<(unsigned)images, 256, 0, stream>>>(ia);

@@ -5,6 +5,11 @@
 //   tc_flush     tensor-core accumulation chain of the single-accumulator
 //                tiles, in stages: 8, 16 (longer chains lose accuracy, so
 //                they are not candidates)
+//   hbin_job_cost  h-binned groups (SPH / Wendland with per-particle radii):
+//                the price of one more h-bin in the bin-count optimisation,
+//                256, 1024 (default), 4096: lower gives more, narrower bins
+//                with fewer Chebyshev nodes per particle, higher fewer jobs
+//                (the accuracy rule on the nodes is the same for all)
 // vis_autotune_spectrum times each candidate on the caller's own data through
 // the public compute path (one warm-up and one timed run, CUDA events on the
 // config's stream), one parameter at a time starting from the defaults, and
@@ -31,6 +36,17 @@ long long dataset_terms(const MeshlessDataset* ds, int* groups) {
     *groups = ds->number_of_groups;
     for (int g = 0; g < ds->number_of_groups; ++g) n += std::max(0, ds->groups[g].number_of_terms);
     return n;
+}
+
+// Whether some group is SPH or Wendland with registered, varying radii (the
+// groups the tensor form takes through h-bins).
+bool dataset_has_varying_radii(const MeshlessDataset* ds) {
+    for (int g = 0; g < ds->number_of_groups; ++g) {
+        const Group& grp = ds->groups[g];
+        if (!grp.d_constraints) continue;
+        if (registered_group_stats(grp.d_constraints).hbins) return true;
+    }
+    return false;
 }
 
 }  // namespace
@@ -87,13 +103,15 @@ int vis_autotune_spectrum(VisSpectrum* sp, VisConfig* vis_config, MeshlessDatase
     };
     TuneParams best;
     float best_t = time_of(best);
-    const int plain_c[] = {2, 4, 6, 8}, waves_c[] = {2, 4, 8}, flush_c[] = {16, 8};
-    for (int field = 0; field < 3 && best_t >= 0.f; ++field) {
-        const int* cand = field == 0 ? plain_c : field == 1 ? waves_c : flush_c;
-        const int count = field == 0 ? 4 : field == 1 ? 3 : 2;
+    const int plain_c[] = {2, 4, 6, 8}, waves_c[] = {2, 4, 8}, flush_c[] = {16, 8}, hbin_c[] = {256, 1024, 4096};
+    const bool binned = dataset_has_varying_radii(meshless_dataset);
+    for (int field = 0; field < 4 && best_t >= 0.f; ++field) {
+        if (field == 3 && !binned) break;
+        const int* cand = field == 0 ? plain_c : field == 1 ? waves_c : field == 2 ? flush_c : hbin_c;
+        const int count = field == 0 ? 4 : field == 1 ? 3 : field == 2 ? 2 : 3;
         for (int i = 0; i < count && best_t >= 0.f; ++i) {
             TuneParams p = best;
-            int& v = field == 0 ? p.plain_waves : field == 1 ? p.tc_waves : p.tc_flush;
+            int& v = field == 0 ? p.plain_waves : field == 1 ? p.tc_waves : field == 2 ? p.tc_flush : p.hbin_job_cost;
             if (v == cand[i]) continue;
             v = cand[i];
             const float t = time_of(p);

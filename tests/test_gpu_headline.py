@@ -3,7 +3,8 @@ measures), against the FP64 oracle (the reference's per-term sum restated in
 FP64, meshless_vis/fourier_transform_cpu.cpp:73-134, on the 3D half-spectrum):
 
   C2  N=262,144 Plummer particles with 32-NN weights and radii, Wendland,
-      128^3 lattice, the plain form and the automatic choice; 1024 points.
+      128^3 lattice, the plain form, the h-binned tensor form and the
+      automatic choice; 1024 points.
   C3  N=2^20 uniform particles, decaying Gaussian with log-uniform h in 16
       h-bins, 256^3 lattice (CTA-pair tensor tiles, B-operand images, the
       Nyquist plane as tensor jobs, 16-stage accumulation chains); the
@@ -48,7 +49,7 @@ def _fp64(groups, step3, ijk):
     return sum(O.spectrum_points(c, r, b, step3, ijk) for c, r, b in groups)
 
 
-@pytest.mark.parametrize("form", [M.FORM_PLAIN, M.FORM_AUTO])
+@pytest.mark.parametrize("form", [M.FORM_PLAIN, M.FORM_AUTO, M.FORM_TENSOR])
 def test_c2_full_size(form):
     w = W.c2()
     spec, _ = spectrum_and_views(w["groups"], w["grid"], w["step3"], w["step"], w["cutoff"], w["samples"], None,
