@@ -42,7 +42,14 @@ typedef struct
     float3 u_axis;
     float3 v_axis;
 
-    bool cull_fully_aliased_terms; /* accepted, ignored (the reference's cull is disabled) */
+    /* false by default (as the reference).  When true,
+     * vis_fourier_volume_rendering sums, per group, only the particles whose
+     * footprint square (centre (p.u, p.v), half-side h_j, 0 without radii)
+     * lies inside [0, 1/(2 step.x)] x [0, 1/(2 step.y)]: the cull of
+     * meshless_vis.cu:39-127, which the reference keeps disabled (:336).  The
+     * registered arrays are left untouched; each render culls from the full
+     * set and waits once per group for the kept count. */
+    bool cull_fully_aliased_terms;
 
     bool _automatic_d_image;
 

@@ -273,6 +273,7 @@ struct ConfigState {
     TensorWorkspace tensor;  // tensor-core form: particle constants, FP64 accumulators, tables
     Workspace post;          // image post-processing (per-image maxima)
     Workspace error_word;  // device int set by kernels that give up a bounded wait
+    Workspace cull;        // kept particles of the aliasing cull
     std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
     KernelTimer timer;
 
@@ -285,6 +286,7 @@ struct ConfigState {
         tensor.release();
         post.release();
         error_word.release();
+        cull.release();
         for (auto& kv : batched_plans) cufftDestroy(kv.second);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -713,6 +715,13 @@ void vis_fourier_volume_rendering(MeshlessDataset* ds, VisConfig* c) {
         r.row = ny / 2 + 1;
         r.accumulate = g > 0;
         r.stream = s->stream;
+        if (c->cull_fully_aliased_terms) {
+            // meshless_vis.cu:336 (disabled there): sum only the particles
+            // whose footprint lies in the cull box, from a compacted copy
+            SumRequest kept;
+            if (cull_aliased_terms(r, c->u_axis, c->v_axis, c->step_size, s->cull, s->stream, &kept) != kOk) return;
+            r = kept;
+        }
         if (launch_plain_sum(r, s->partials, &s->timer) != kOk) return;
     }
     if (check_cufft(cufftSetStream(c->_plan, s->stream), "cufftSetStream") != kOk) return;

@@ -99,6 +99,12 @@ struct KernelTimer;  // per-stage event pairs, see mv_api.cu
 // Plain FP32 form.  Uses `ws` for split-K partial sums.
 int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer);
 
+// Aliasing cull of the direct path (mv_cull.cu): `out` is `in` restricted to
+// the particles whose footprint in the view (u, v) lies in [0, 1/(2 step.x)] x
+// [0, 1/(2 step.y)], compacted in order into `ws`; waits for the kept count.
+int cull_aliased_terms(const SumRequest& in, float3 u, float3 v, float2 step, Workspace& ws, cudaStream_t stream,
+                       SumRequest* out);
+
 // Slice extraction for a batch of views into the C2R layout
 // [views][nx][ny/2+1].  views: device array of 8 floats per view
 // (u.x, u.y, u.z, v.x, v.y, v.z, step.x, step.y).

@@ -1457,11 +1457,20 @@ long long lattice_nsq(const Lattice& L) {
     return hx * hx + hy * hy + hz * hz;
 }
 
+// Work per particle of a bin of Chebyshev order P whose blocks are `period`
+// columns wide: the A operand is produced once per n-tile (at most 128 c
+// values), the MMAs scale with the columns; both in units of one full n-tile.
+double hbin_unit_cost(int order, int period) {
+    const double tiles = (double)order * period / Shape<kWide>::kNc;
+    return std::ceil(tiles) + tiles;
+}
+
 // Bins of a group on a lattice: runs of fine bins chosen by dynamic
-// programming to minimise sum(count x order) + job_cost per non-empty bin
-// (a bin is one more job: its items, pipeline fills and accumulator dumps),
-// each bin's Chebyshev interval the span of its non-empty fine bins.
-HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int job_cost) {
+// programming to minimise sum(count x hbin_unit_cost) + job_cost per
+// non-empty bin (a bin is one more job: its items, pipeline fills and
+// accumulator dumps), each bin's Chebyshev interval the span of its non-empty
+// fine bins.
+HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_cost) {
     const int F = kHBinFine;
     std::vector<long long> cum(F + 1, 0);
     for (int f = 0; f < F; ++f) cum[f + 1] = cum[f] + hs.count[f];
@@ -1480,7 +1489,7 @@ HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int job_cost) {
                 order = hbin_order(kmax * dh);
                 if (order > kHBinMaxOrder) break;  // wider runs only need more
             }
-            const double c = best[i] + (double)n * order + (n > 0 ? job_cost : 0);
+            const double c = best[i] + (double)n * hbin_unit_cost(order, period) + (n > 0 ? job_cost : 0);
             if (c < best[j]) {
                 best[j] = c;
                 arg[j] = i;
@@ -1529,12 +1538,13 @@ std::shared_ptr<const HBinPlan> hbin_plan(const SumRequest& r) {
     const long long nsq = lattice_nsq(r.lat);
     const double kmax = r.lat.kx * std::sqrt((double)nsq);
     const int job_cost = std::max(0, active_tune().hbin_job_cost);
-    const auto key = std::make_tuple(r.hbins->id, nsq, r.lat.kx, job_cost);
+    const int period = r.lat.nz - 1;
+    const auto key = std::make_tuple(r.hbins->id, nsq * 65536 + period, r.lat.kx, job_cost);
     std::lock_guard<std::mutex> lock(g_hbin_mu);
     auto it = g_hbin_cache.find(key);
     if (it != g_hbin_cache.end()) return it->second;
     if (g_hbin_cache.size() >= 256) g_hbin_cache.clear();
-    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, job_cost));
+    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, period, job_cost));
     g_hbin_cache[key] = plan;
     return plan;
 }

@@ -161,6 +161,28 @@ def render_from_spectrum(spec, grid, step3, step, cutoff, views, samples):
     return np.stack([c2r(extract_slice(spec, grid, step3, step, cutoff, u, v, samples), samples) for u, v in views])
 
 
+def cull_mask(cons, radii, u, v, step):
+    """The aliasing cull's keep mask, as meshless_vis/meshless_vis.cu:39-57
+    (compute_mask, point_in_box) with the box of :88-89: a particle is kept
+    when its footprint square, centre (p.u, p.v) and half-side h (0 without
+    radii), lies inside [0, 1/(2 step.x)] x [0, 1/(2 step.y)].  Computed in
+    FP32 as the reference does."""
+    xyzw = _xyzw(cons)
+    p = xyzw[:, :3].astype(np.float32)
+    u = np.asarray(u, np.float32)
+    v = np.asarray(v, np.float32)
+    cx = (p[:, 0] * u[0] + p[:, 1] * u[1] + p[:, 2] * u[2]).astype(np.float32)
+    cy = (p[:, 0] * v[0] + p[:, 1] * v[1] + p[:, 2] * v[2]).astype(np.float32)
+    r = np.zeros(len(p), np.float32) if radii is None else _f32(radii)
+    bx = np.float32(0.5) / np.float32(step[0])
+    by = np.float32(0.5) / np.float32(step[1])
+    keep = np.ones(len(p), bool)
+    for xs in (cx + r, cx - r):
+        for ys in (cy + r, cy - r):
+            keep &= (xs >= 0) & (ys >= 0) & (xs <= bx) & (ys <= by)
+    return keep
+
+
 def rel_l2(a, b):
     a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64)
     b = np.asarray(b, dtype=a.dtype)

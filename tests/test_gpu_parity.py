@@ -470,3 +470,39 @@ def test_device_shift_matches_host_shift():
     shifted = constraints(pos - np.float32(5.0), cons["weight"])
     ref = O.render_direct([(shifted, radii, M.SPH)], (0.1, 0.1), (16, 16), (1, 0, 0), (0, 1, 0), (64, 64))
     assert O.rel_l2(img, ref) < SPEC_TOL
+
+
+# ------------------------------------------------------------ aliasing cull
+@pytest.mark.parametrize("with_radii", [True, False])
+def test_aliasing_cull_sums_only_the_kept_particles(with_radii):
+    """cull_fully_aliased_terms (meshless_vis.cu:39-127, disabled in the
+    reference): with the flag set, the direct render equals the FP64 render of
+    the particles the oracle's mask keeps (about half of them here, in two
+    groups); the registered arrays are untouched, so clearing the flag renders
+    the full set again."""
+    rng = np.random.default_rng(91)
+    step, cutoff, samples = (0.1, 0.1), (16, 16), (64, 64)
+    u, v = (0.8, 0.0, -0.6), (0.0, 1.0, 0.0)
+    groups = []
+    for basis, n in ((M.SPH, 3001), (M.WENDLAND_D3_C2, 2500)):
+        pos = (rng.random((n, 3), dtype=np.float32) * 8.0 - 1.0).astype(np.float32)
+        radii = np.exp(rng.uniform(np.log(0.1), np.log(0.6), n)).astype(np.float32) if with_radii else None
+        groups.append((constraints(pos, rng.standard_normal(n).astype(np.float32)), radii, basis))
+    kept = []
+    for cons, radii, basis in groups:
+        m = O.cull_mask(cons, radii, u, v, step)
+        assert 0.2 < m.mean() < 0.8
+        kept.append((cons[m], None if radii is None else radii[m], basis))
+    cfg = M.Config(step=step, cutoff=cutoff, u=u, v=v, samples=samples, block_length=64)
+    ds = to_dataset(groups)
+    cfg.register(ds)
+    cfg.c.cull_fully_aliased_terms = True
+    cfg.render(ds)
+    culled = cfg.image()
+    cfg.c.cull_fully_aliased_terms = False
+    cfg.render(ds)
+    full = cfg.image()
+    cfg.unregister(ds)
+    cfg.close()
+    assert O.rel_l2(culled, O.render_direct(kept, step, cutoff, u, v, samples)) < SPEC_TOL
+    assert O.rel_l2(full, O.render_direct(groups, step, cutoff, u, v, samples)) < SPEC_TOL

@@ -110,3 +110,20 @@ def test_reference_build_runs_and_matches_oracle_live():
     img = R.render()
     R.close()
     assert O.rel_l2(img, O.render_direct(groups, (1.0, 1.0), (8, 8), (1, 0, 0), (0, 1, 0), (16, 16))) < 2e-5
+
+
+def test_cull_mask_known_answers():
+    """meshless_vis.cu:39-57: kept when the footprint square lies in
+    [0, 1/(2 step.x)] x [0, 1/(2 step.y)] (step 0.1: the box is [0, 5]^2)."""
+    from libmeshlessvis_b200.workloads import constraints
+
+    pos = np.array([[1, 1, 9], [4.9, 2, 0], [4.9, 2, 0], [-0.1, 1, 0], [2, 5.2, 0], [0.3, 0.3, 0]], np.float32)
+    radii = np.array([0.5, 0.2, 0.05, 0.01, 0.1, 0.3], np.float32)
+    cons = constraints(pos, np.ones(len(pos), np.float32))
+    keep = O.cull_mask(cons, radii, (1, 0, 0), (0, 1, 0), (0.1, 0.1))
+    assert keep.tolist() == [True, False, True, False, False, True]
+    # without radii the footprint is the centre
+    assert O.cull_mask(cons, None, (1, 0, 0), (0, 1, 0), (0.1, 0.1)).tolist() == [True, True, True, False, False, True]
+    # a rotated view projects z onto u
+    keep = O.cull_mask(cons, None, (0, 0, 1), (0, 1, 0), (0.1, 0.1))
+    assert keep.tolist() == [False, True, True, True, False, True]
