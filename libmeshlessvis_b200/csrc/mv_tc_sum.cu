@@ -603,15 +603,26 @@ __device__ __noinline__ void dump_binned(const TcItem& I, const float* tt, int c
     const int ab2 = a_f * a_f + b_f * b_f;
     const float* coef = I.job->coef;
     const int stride = I.job->coef_stride;
-    for (int i = 0; i < 32; ++i) {
-        const int n = cc + i;
-        if (n >= ncols) break;
-        const int h = n / half_cols, nn = n - h * half_cols;
-        const int im = nn >= I.bnc ? 1 : 0;
-        const int c = I.c0 + h * I.bnc + nn - im * I.bnc;
-        const int q = c / I.period, cf = c - q * I.period, cfreq = cf + I.c_base;
-        const double w = (double)__ldg(coef + (size_t)q * stride + ab2 + cfreq * cfreq);
-        atomicAdd(acc + (size_t)(2 * cf + im) * mk + rho, (double)tt[i] * dump_scale * w);
+    // in batches of 8 columns: every coefficient load of a batch is issued
+    // before the first is used, so their L2 latencies overlap
+#pragma unroll 1
+    for (int i0 = 0; i0 < 32; i0 += 8) {
+        float w[8];
+        int dst[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int n = min(cc + i0 + i, ncols - 1);  // columns past ncols: loaded, not added
+            const int h = n / half_cols, nn = n - h * half_cols;
+            const int im = nn >= I.bnc ? 1 : 0;
+            const int c = I.c0 + h * I.bnc + nn - im * I.bnc;
+            const int q = c / I.period, cf = c - q * I.period, cfreq = cf + I.c_base;
+            w[i] = __ldg(coef + (size_t)q * stride + ab2 + cfreq * cfreq);
+            dst[i] = 2 * cf + im;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (cc + i0 + i < ncols)
+                atomicAdd(acc + (size_t)dst[i] * mk + rho, (double)tt[i0 + i] * dump_scale * (double)w[i]);
     }
 }
 
@@ -816,25 +827,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                             tt[i + 1] = t2.y;
                         }
                     }
-                    if (!dump) {
-                        tmem_st32(lane_base + kColTotal + cc, tt);
-                    } else if (I.period == 0) {
-                        // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows are
-                        // contiguous.  Column n: CTA h = n / half_cols's B rows,
-                        // Re then Im of its bnc c values.
-#pragma unroll
-                        for (int i = 0; i < 32; ++i) {
-                            const int n = cc + i;
-                            if (n < ncols && in_rows) {
-                                const int h = n / half_cols, nn = n - h * half_cols;
-                                const int im = nn >= I.bnc ? 1 : 0;
-                                const int c = c0 + h * I.bnc + nn - im * I.bnc;
-                                atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
-                            }
-                        }
-                    } else {
-                        dump_binned(I, tt, cc, ncols, half_cols, rho, in_rows, mk, acc, dump_scale);
-                    }
+                    tmem_st32(lane_base + kColTotal + cc, tt);
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -844,6 +837,34 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     // own warps arrive locally
                     if (rank == 0) mbar_arrive(&acc_empty[b]);
                     else mbar_arrive_leader(&acc_empty[b]);
+                }
+                if (dump) {
+                    // the total is read back from its own TMEM columns, which
+                    // the MMAs never write: the dump overlaps the next chain
+                    tmem_wait_st();
+#pragma unroll 1
+                    for (int cc = 0; cc < ncols; cc += 32) {
+                        float tt[32];
+                        tmem_ld32(lane_base + kColTotal + cc, tt);
+                        tmem_wait_ld();
+                        if (I.period == 0) {
+                            // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows
+                            // are contiguous.  Column n: CTA h = n / half_cols's B
+                            // rows, Re then Im of its bnc c values.
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) {
+                                const int n = cc + i;
+                                if (n < ncols && in_rows) {
+                                    const int h = n / half_cols, nn = n - h * half_cols;
+                                    const int im = nn >= I.bnc ? 1 : 0;
+                                    const int c = c0 + h * I.bnc + nn - im * I.bnc;
+                                    atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
+                                }
+                            }
+                        } else {
+                            dump_binned(I, tt, cc, ncols, half_cols, rho, in_rows, mk, acc, dump_scale);
+                        }
+                    }
                 }
             }
             C += I.n_chunks;
@@ -1426,18 +1447,25 @@ namespace {
 
 // ---------------------------------------------------------------- h-bins
 // Chebyshev order of a bin whose radii span dh at the lattice's largest |k|:
-// the smallest P with 2 (pi x / 4)^P / P! <= kHBinTau, x = |k|max dh (the
-// interpolation error bound of an oscillation of that frequency, with the
-// constant set on the sums' FP64 error: about 1e-6 rel-L2 on SPH and Wendland
-// sets with 58x ranges of h); bins needing more than kHBinMaxOrder nodes are
-// not formed.
-constexpr double kHBinTau = 3e-6;
+// the smallest P with 2 (pi x / 2)^P / P! <= kHBinTau, x = |k|max dh.  That is
+// the interpolation error bound for h -> Phi^(|k| h), whose P-th derivative is
+// at most (2 pi |k|)^P Phi^(0) (the basis functions have support radius h);
+// bins needing more than kHBinMaxOrder nodes are not formed.
+constexpr double kHBinTau = 3e-5;
 constexpr int kHBinMaxOrder = 12;
+// The reference's Phi^ switches from a quadratic fit to the closed form at a
+// branch point r0 (0.06 SPH, 0.24 Wendland; fourier_transform.cu:33, :50),
+// where its slope jumps by 0.4% (SPH) and 1.3% (Wendland) of Phi^(0).  No
+// polynomial in h follows that kink, so a bin whose |k| h reaches r0 on the
+// lattice is kept at most kHBinKinkWidth wide (hi / lo - 1): the kink then
+// costs a few 1e-7 of the sum (CPU models of the scheme against the oracle's
+// FP64 Phi^: C2's set 6e-8, uniform sets with h in [0.01, 0.05] up to 7e-7).
+constexpr double kHBinKinkWidth = 0.05;
 
 double hbin_order_limit(int order) {  // largest x that `order` nodes cover
     double f = 1.0;
     for (int i = 2; i <= order; ++i) f *= i;
-    return (4.0 / kPi) * std::pow(kHBinTau * f / 2.0, 1.0 / order);
+    return (2.0 / kPi) * std::pow(kHBinTau * f / 2.0, 1.0 / order);
 }
 
 int hbin_order(double x) {
@@ -1450,6 +1478,8 @@ int hbin_order(double x) {
         if (x <= limit[p]) return p;
     return kHBinMaxOrder + 1;
 }
+
+double hbin_branch_point(int basis) { return basis == kSph ? (double)0.06f : (double)0.24f; }
 
 // The largest |k| of a half-spectrum lattice and the largest a^2 + b^2 + c^2.
 long long lattice_nsq(const Lattice& L) {
@@ -1470,7 +1500,8 @@ double hbin_unit_cost(int order, int period) {
 // non-empty bin (a bin is one more job: its items, pipeline fills and
 // accumulator dumps), each bin's Chebyshev interval the span of its non-empty
 // fine bins.
-HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_cost) {
+HBinPlan hbin_plan_build(const HBinStats& hs, int basis, double kmax, int period, int job_cost) {
+    const double r0 = hbin_branch_point(basis);
     const int F = kHBinFine;
     std::vector<long long> cum(F + 1, 0);
     for (int f = 0; f < F; ++f) cum[f + 1] = cum[f] + hs.count[f];
@@ -1485,9 +1516,11 @@ HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_c
             const long long n = cum[j] - cum[i];
             int order = 1;
             if (n > 0) {
-                const double dh = (double)hs.edges[last_ne[j] + 1] - (double)hs.edges[first_ne[i]];
-                order = hbin_order(kmax * dh);
-                if (order > kHBinMaxOrder) break;  // wider runs only need more
+                const double lo = hs.edges[first_ne[i]], hi = hs.edges[last_ne[j] + 1];
+                order = hbin_order(kmax * (hi - lo));
+                // wider runs (smaller i) only need more nodes and are wider still
+                if (order > kHBinMaxOrder) break;
+                if (kmax * hi > r0 && hi > lo * (1.0 + kHBinKinkWidth)) break;
             }
             const double c = best[i] + (double)n * hbin_unit_cost(order, period) + (n > 0 ? job_cost : 0);
             if (c < best[j]) {
@@ -1537,14 +1570,20 @@ std::map<std::tuple<unsigned long long, long long, double, int>, std::shared_ptr
 std::shared_ptr<const HBinPlan> hbin_plan(const SumRequest& r) {
     const long long nsq = lattice_nsq(r.lat);
     const double kmax = r.lat.kx * std::sqrt((double)nsq);
-    const int job_cost = std::max(0, active_tune().hbin_job_cost);
+    // MV_HBIN_JOB_COST (0 .. 1e6) replaces the tuned price of one more bin
+    static const int env_cost = [] {
+        const char* e = std::getenv("MV_HBIN_JOB_COST");
+        const long v = e ? std::atol(e) : -1;
+        return (v >= 0 && v <= 1000000) ? (int)v : -1;
+    }();
+    const int job_cost = env_cost >= 0 ? env_cost : std::max(0, active_tune().hbin_job_cost);
     const int period = r.lat.nz - 1;
-    const auto key = std::make_tuple(r.hbins->id, nsq * 65536 + period, r.lat.kx, job_cost);
+    const auto key = std::make_tuple(r.hbins->id, (nsq * 65536 + period) * 4 + r.basis, r.lat.kx, job_cost);
     std::lock_guard<std::mutex> lock(g_hbin_mu);
     auto it = g_hbin_cache.find(key);
     if (it != g_hbin_cache.end()) return it->second;
     if (g_hbin_cache.size() >= 256) g_hbin_cache.clear();
-    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, period, job_cost));
+    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, r.basis, kmax, period, job_cost));
     g_hbin_cache[key] = plan;
     return plan;
 }
@@ -1609,6 +1648,9 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         int mode;
         long long cost;
         int2 item;
+        int m_tile;  // for the order below
+        int split;
+        int cost_class = 0, m_block = 0;
     };
     std::vector<Item> items;
     plan.flush_narrow = tc_flush_stages(kNarrow);
@@ -1661,7 +1703,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
             const long long stages = (k1 - k0 + kKp - 1) / kKp;
             for (long long t = 0; t < ftiles; ++t)
-                items.push_back({mode, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t))});
+                items.push_back({mode, stages + (stages + flush - 1) / flush, make_int2(job_index, (int)(ks * ftiles + t)),
+                                 (int)(t / j.n_ntiles), (int)ks});
         }
         return job_index;
     };
@@ -1844,10 +1887,25 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         }
     }
     if (items.size() > (size_t)INT32_MAX) return set_error(kInvalidValue, "tensor sum: too many work items");
-    // per tile mode, longest first (round-robin over the persistent CTAs / pairs)
+    // Per tile mode, longest first (round-robin over the persistent CTAs /
+    // pairs), in cost classes 5% wide.  Within a class, items run in blocks of
+    // as many m-tiles as there are resident units: one wave takes one (job,
+    // split) over distinct m-tiles, and the next waves the other jobs' items of
+    // the same m-tiles, so jobs that share an FP64 accumulator (the h-bins of a
+    // spectrum) dump into lines still held in L2 instead of re-reading them.
     auto order = [](int m) { return m == kNarrow ? 0 : m == kPairNarrow ? 1 : m == kPair ? 2 : 3; };
+    const int sms = std::max(2, device_sm_count());
+    for (Item& it : items) {
+        it.cost_class = (int)std::floor(std::log((double)std::max(1LL, it.cost)) / std::log(1.05));
+        it.m_block = it.m_tile / (pair_mode(it.mode) ? sms / 2 : sms);
+    }
     std::stable_sort(items.begin(), items.end(), [&](const Item& x, const Item& y) {
-        return x.mode != y.mode ? order(x.mode) < order(y.mode) : x.cost > y.cost;
+        if (x.mode != y.mode) return order(x.mode) < order(y.mode);
+        if (x.cost_class != y.cost_class) return x.cost_class > y.cost_class;
+        if (x.m_block != y.m_block) return x.m_block < y.m_block;
+        if (x.item.x != y.item.x) return x.item.x < y.item.x;
+        if (x.split != y.split) return x.split < y.split;
+        return x.item.y < y.item.y;
     });
     plan.items.reserve(items.size());
     plan.n_narrow = plan.n_pair_narrow = plan.n_pair = 0;
