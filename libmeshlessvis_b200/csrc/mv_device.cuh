@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "phi_poly.h"
+#include "phi_series.h"
 
 namespace mv {
 
@@ -92,6 +93,45 @@ __device__ __forceinline__ double phi_fp64(int basis, double r) {
         return 0.299199300341890 + r * (-0.002379178586124 + r * (-0.370530218163545));
     default: return exp(-kPi * r * r);
     }
+}
+
+// The reference's branch point of SPH (0.06f) and Wendland (0.24f).
+__host__ __device__ __forceinline__ double phi_branch_point(int basis) {
+    return basis == kSph ? (double)0.06f : (double)0.24f;
+}
+
+// SPH and Wendland without the branch: the closed form at every r (smooth),
+// from its power series below the branch point (phi_series.h), where the
+// closed form cancels, and the closed form above.
+__device__ __forceinline__ double phi_smooth_fp64(int basis, double r) {
+    if (r >= phi_branch_point(basis)) return phi_fp64(basis, r);
+    const double m = kPi * r, m2 = m * m;
+    const double* c = basis == kSph ? MV_SPH_SERIES : MV_WENDLAND_SERIES;
+    double acc = c[MV_PHI_SERIES_TERMS - 1];
+    for (int n = MV_PHI_SERIES_TERMS - 2; n >= 0; --n) acc = fma(acc, m2, c[n]);
+    return (basis == kSph ? 2.3561944901923448 : kPi * 7.5) * acc;
+}
+
+// What the branch adds: the reference's quadratic fit minus the smooth closed
+// form below the branch point, zero above (Phi^ = smooth + kink).
+__device__ __forceinline__ double phi_kink_fp64(int basis, double r) {
+    if (r >= phi_branch_point(basis)) return 0.0;
+    return phi_fp64(basis, r) - phi_smooth_fp64(basis, r);
+}
+
+// Bin of radius h among nb bins with edges e[0..nb]: the largest i with
+// e[i] <= h, clamped to [0, nb) (the h-binned tensor form's classification;
+// the same rule at registration sizes the bins).
+__device__ __forceinline__ int hbin_of(const float* e, int nb, float h) {
+    if (nb <= 1 || !(h >= e[1])) return 0;
+    if (h >= e[nb - 1]) return nb - 1;
+    int lo = 0, hi = nb;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (e[mid] <= h) lo = mid;
+        else hi = mid;
+    }
+    return lo;
 }
 
 // Fixed-point turn count of q (in turns): round(q * 2^32) mod 2^32.  Exact for

@@ -84,6 +84,15 @@ struct SumRequest {
     bool accumulate;
     cudaStream_t stream;
     int* error_flag;  // device word set by kernels that give up a bounded wait
+    // The branch part of an h-binned group (SPH / Wendland): kink = 1 sums
+    // Phi^ minus its smooth closed form (nonzero below the branch point r0)
+    // over particles sorted into shell_nbins h-bins (classification edges
+    // shell_edges, first particles shell_first, both device arrays), at each
+    // frequency k over the particles of the one bin that holds r0 / |k|.
+    int kink;
+    const float* shell_edges;
+    const int* shell_first;
+    int shell_nbins;
 };
 
 // Grow-only device scratch owned by one VisConfig.
@@ -141,12 +150,14 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 
 // Tensor-core form (mv_tc_sum.cu).  A set of groups -- of one or several
 // half-spectra -- is summed by one persistent tcgen05 launch:
-//   tensor_plan           host only: jobs, work items, accumulator classes;
+//   tensor_plan           host only: jobs, work items, output classes;
 //   tensor_reserve_upload grows the workspaces and uploads the job and item
 //                         tables (not capturable in a CUDA graph);
-//   tensor_enqueue        memsets, per-particle constants, the persistent
-//                         launch, FP64 -> spectrum (added), the Nyquist planes
-//                         of groups without a Nyquist job (plain form, added);
+//   tensor_enqueue        per-particle constants, the persistent launch (each
+//                         work item stores its FP32 tile), the FP64 reduction
+//                         of the tiles into the spectra (added), the Nyquist
+//                         planes of groups without a Nyquist job and the
+//                         branch part of h-binned groups (plain form, added);
 //                         stream-ordered and capturable once the workspaces
 //                         are large enough.
 // The spectra must be zeroed (or hold earlier groups) before tensor_enqueue.
@@ -156,7 +167,7 @@ int tensor_sum_available(const SumRequest& req, int form);
 // One job of the persistent tensor-core kernel: a separable group summed over
 // a lattice of rows (a, b) and columns c >= 0 into an FP64 accumulator.  Its
 // work items are (split ks, m tile, n tile), local index (ks * n_mtiles +
-// m_tile) * n_ntiles + n_tile.  Device-resident (104 bytes).
+// m_tile) * n_ntiles + n_tile.  Device-resident.
 //
 // Frequencies: a = a_idx + a_base, b = b_idx + b_base, c = c_idx + c_base.
 // A group's planes c < Kz/2 are one job (a_base = -Kx/2, b_base = -Ky/2,
@@ -176,7 +187,15 @@ int tensor_sum_available(const SumRequest& req, int form);
 // per stage.
 struct TcJob {
     const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
-    double* acc;           // [c_idx][Re, Im][a_idx * ky + b_idx]
+    // Item results: each work item stores its FP32 tile once, at its end, into
+    // slots[local item * slot_stride ..]: per CTA of the item (rank r at
+    // r * 128 * 2 nc_tile) its 128 rows of every accumulator column n, in
+    // quads of columns: [n / 4][row][n % 4].
+    // tc_reduce_kernel sums them over the items of every job in FP64.
+    float* slots;
+    int slot_stride;  // floats per item: ctas * 128 * 2 nc_tile
+    int n_splits;     // particle chunks (items per tile)
+    int ctas;         // 2 for the CTA-pair tiles
     double wmax;
     int kx, ky, lz_tc;  // row extents (a_idx < kx, b_idx < ky); columns c_idx < lz_tc
     int n_mtiles, n_ntiles;
@@ -193,13 +212,17 @@ struct TcJob {
     // h-binned jobs (period > 0): the job's lz_tc = P x period columns are P
     // blocks of `period` frequency columns, block q weighted on the B side by
     // the Chebyshev polynomial T_q(t_j) of the particle's normalised radius t_j
-    // in its bin (kept in the constants' gam field).  Each dumped value is
-    // multiplied by coef[q * coef_stride + a^2 + b^2 + c^2], the q-th Chebyshev
-    // coefficient of h -> Phi^(|k| h) over the bin, and added into the
-    // accumulator column c = column % period.
+    // in its bin (kept in the constants' gam field).  The reduction multiplies
+    // block q's value at frequency column c by coef[(a^2 + b^2 + c^2) *
+    // coef_stride + q], the q-th Chebyshev coefficient of h -> Phi^(|k| h)
+    // over the bin (the group's table holds all its bins' q for one |k|^2
+    // together).
     const float* coef;
     int period;
     int coef_stride;
+    // the slot column of job column c (tc_reduce_kernel): (n-tile, Re column,
+    // Im column, 0) per column
+    const int4* colmap;
 };
 
 // The h-bins of one binned group on one lattice (tensor_plan): consecutive
@@ -229,10 +252,13 @@ struct TensorPlan {
         size_t cursor_offset;   // into acc (ints)
         size_t coef_offset;     // into coef (floats)
         size_t coef_count;
-        int nsq;                // coefficient table stride: max a^2 + b^2 + c^2 + 1
+        int nsq;                // |k|^2 / step^2 values: max a^2 + b^2 + c^2 + 1
+        int total_q;            // Chebyshev blocks over all bins: the table's stride per |k|^2
         std::vector<HBin> bins;
         std::vector<float> edges;  // nbins + 1: the fine edges where the bins start (classification)
+        size_t sorted_offset;      // into TensorWorkspace::sorted: n float4, then n radii (256-aligned)
     };
+    size_t sorted_bytes = 0;
     std::vector<Binned> binned;
     size_t coef_bytes = 0;
     struct Class {
@@ -243,9 +269,10 @@ struct TensorPlan {
         double h;
         bool factored;
         double scale;
-        size_t acc_offset;
-        bool nyquist;             // the Nyquist plane is summed by the groups' transposed jobs
-        size_t acc_nyq_offset;    // their FP64 accumulator: the a < 0 job's columns, then the a >= 0 job's
+        bool nyquist;  // the Nyquist plane is summed by the groups' transposed jobs
+        // the class's jobs (indices into jobs): planes, Nyquist a >= 0, Nyquist a < 0
+        std::vector<int> jobs, nyq_pos, nyq_neg;
+        size_t list_offset = 0;  // those three lists in meta (ints)
     };
     std::vector<TcJob> jobs;
     std::vector<int2> items;  // 128x128-tile items (n_narrow), narrow CTA-pair items (n_pair_narrow),
@@ -258,8 +285,15 @@ struct TensorPlan {
     // per job: its particle constants (offset into the particles workspace),
     // accumulator class and part (0 planes, 1 Nyquist a >= 0, 2 Nyquist a < 0),
     // coefficient table (offset in floats into coef, SIZE_MAX for none)
-    std::vector<size_t> job_tp, job_coef;
+    std::vector<size_t> job_tp, job_coef, job_slot;  // job_slot: offset in floats into slots
+    std::vector<size_t> job_colmap;                 // the job's column map: index into colmaps
+    std::vector<int4> colmaps;                      // all jobs' column maps
+    size_t colmap_offset = 0;                       // colmaps in meta
+    std::vector<int> img_jobs;                      // the jobs with B-operand images
+    std::vector<long long> img_first;               // their first images (and the total last)
+    size_t img_jobs_offset = 0, img_first_offset = 0;  // both in meta
     std::vector<int> job_class, job_acc;
+    size_t slot_floats = 0;
     std::vector<size_t> tp_offset, tp_nyq_offset;
     std::vector<size_t> bimg_offset;  // per job: its B-operand images in the workspace, or SIZE_MAX
     size_t bimg_bytes = 0;
@@ -272,10 +306,12 @@ struct TensorPlan {
 
 struct TensorWorkspace {
     Workspace particles;  // per-particle constants of every group
-    Workspace acc;        // FP64 accumulators
+    Workspace acc;        // per-compute counters (zeroed each compute)
+    Workspace slots;      // work items' FP32 tiles
     Workspace meta;       // job and item tables
     Workspace bimg;       // B-operand images
     Workspace coef;       // Chebyshev coefficient tables of h-binned groups
+    Workspace sorted;     // h-binned groups' particles and radii sorted by bin
     std::vector<char> uploaded;  // the tables last copied to `meta`
     void* uploaded_to = nullptr;
     void release() {
@@ -283,9 +319,11 @@ struct TensorWorkspace {
         uploaded_to = nullptr;
         particles.release();
         acc.release();
+        slots.release();
         meta.release();
         bimg.release();
         coef.release();
+        sorted.release();
     }
 };
 
@@ -313,7 +351,8 @@ struct TuneParams {
     int tc_waves = 4;     // tensor form: particle splits until the items make ~tc_waves waves
     int tc_flush = 16;    // tensor form, single-accumulator tiles: stages per TMEM chain (8 or 16;
                           // the double-buffered 128x128 tile uses at most 8)
-    int hbin_job_cost = 1024;  // h-binned groups: cost of one more bin (a job), in particle x node units
+    int hbin_job_cost = 1024;  // h-binned groups: cost of one more bin (a job), in particle x n-tile units
+    int hbin_block_cost = 0;  // h-binned groups: cost of one more Chebyshev block (the reduction), same units
 };
 // The parameters in force on this thread: set by TuneScope around a compute.
 const TuneParams& active_tune();

@@ -40,6 +40,8 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "meshless.h"
 #include "mv_device.cuh"
@@ -58,7 +60,11 @@ constexpr int kMaxTable = 4096;  // cubic cells held in shared memory (64 KB)
 // g(x+1) = g(x) q(x), q(x+1) = q(x) exp(-2 pi h^2).  An x factor that
 // underflows FP32 stays below 1e-28 over 8 steps, so nothing significant is
 // lost.
-enum Amp : int { kAmpFactored = 0, kAmpTable = 1, kAmpExp2 = 2, kAmpGaussRec = 3 };
+// kAmpShell: the branch part of an h-binned group (fold kernel only): the
+// table holds Phi^ minus its smooth closed form (zero from the branch point
+// on), particles come sorted by h-bin, and a term counts only when the
+// particle's bin is the one holding r0 / |k| (see fold_sum_kernel).
+enum Amp : int { kAmpFactored = 0, kAmpTable = 1, kAmpExp2 = 2, kAmpGaussRec = 3, kAmpShell = 4 };
 
 struct SumKernelArgs {
     const float4* particles;
@@ -252,32 +258,57 @@ struct FoldKernelArgs {
     int yrows;     // FY == 2: YP representatives yp; FY == 1: lat.ny
     size_t plane;  // partial sums per split: lat.nx * n_rest
     double2* sums;  // [split][L * 2 FY][gridDim.x * kThreads] running FP64 sums
+    // kAmpShell: particles sorted into shell_nbins h-bins (classification
+    // edges, first particle of each bin) and the branch point r0
+    int shell_nbins;
+    const float* shell_edges;
+    const int* shell_first;
+    float shell_r0;
+    const uint32_t* shell_reps;  // representatives sorted by |k|: x | y << 10 | z << 20
+    int shell_count;
 };
 
 template <int L, int FY, int AMP>
 __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa) {
     const SumKernelArgs& a = fa.s;
-    extern __shared__ float4 s_tab[];  // table cells (kAmpTable only)
+    constexpr bool kShell = AMP == kAmpShell;
+    constexpr bool kTab = AMP == kAmpTable || kShell;
+    extern __shared__ float4 s_tab[];  // table cells (kAmpTable, kAmpShell)
     __shared__ uint4 s_q[kThreads];    // Qx, Qy, Qz, weight bits
     __shared__ float2 s_rot[kThreads];  // exp(2 pi i Qx / 2^32)
     __shared__ float s_h[kThreads];    // per-particle amplitude parameter
+    __shared__ int s_bin[kShell ? kThreads : 1];  // kAmpShell: the particle's h-bin
 
     const int tid = threadIdx.x;
-    if constexpr (AMP == kAmpTable) {
+    if constexpr (kTab) {
         for (int i = tid; i <= a.table_n; i += kThreads) s_tab[i] = a.table[i];
     }
 
     const int nz = a.lat.nz;
     const long long n_rest_f = (long long)fa.yrows * nz;
     const long long t = (long long)blockIdx.x * kThreads + tid;
-    const bool active = t < (long long)fa.xpc * n_rest_f;
-    const int xc = active ? (int)(t / n_rest_f) : 0;
-    const int rf = active ? (int)(t % n_rest_f) : 0;
-    const int yp = FY == 2 ? rf / nz : a.lat.y0 + rf / nz;
-    const int z = a.lat.z0 + rf % nz;
+    bool active;
+    int xc, yr, zr;
+    if constexpr (kShell) {
+        // one representative per thread (L == 1), from the list sorted by |k|:
+        // a warp's 32 have nearly the same |k|, hence the same h-bin or two
+        active = t < fa.shell_count;
+        const uint32_t e = active ? fa.shell_reps[t] : 0u;
+        xc = (int)(e & 1023u);
+        yr = (int)((e >> 10) & 1023u);
+        zr = (int)(e >> 20);
+    } else {
+        active = t < (long long)fa.xpc * n_rest_f;
+        xc = active ? (int)(t / n_rest_f) : 0;
+        const int rf = active ? (int)(t % n_rest_f) : 0;
+        yr = rf / nz;
+        zr = rf % nz;
+    }
+    const int yp = FY == 2 ? yr : a.lat.y0 + yr;
+    const int z = a.lat.z0 + zr;
     const int xb = xc * L;
 
-    // |k| (kAmpTable) or |k|^2 (kAmpExp2) of the thread's L representatives.
+    // |k| (table kinds) or |k|^2 (kAmpExp2) of the thread's L representatives.
     float r[L];
     if constexpr (AMP != kAmpFactored) {
         const double ry = a.lat.ky * yp, rz = a.lat.kz * z;
@@ -285,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
         for (int m = 0; m < L; ++m) {
             const double rx = a.lat.kx * (xb + m);
             const double r2 = rx * rx + ry * ry + rz * rz;
-            r[m] = AMP == kAmpTable ? (float)sqrt(r2) : (float)r2;
+            r[m] = kTab ? (float)sqrt(r2) : (float)r2;
         }
     }
 
@@ -293,8 +324,43 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
     const size_t tstride = (size_t)gridDim.x * kThreads;
     double2* sums = fa.sums + (size_t)blockIdx.y * (L * NP) * tstride + t;  // this thread's, stride tstride
 
-    const int beg = blockIdx.y * a.chunk;
-    const int end = min(a.n, beg + a.chunk);
+    // kAmpShell: at frequency k only the particles of the h-bin holding
+    // r0 / |k| count (the tensor form takes the closed form for that bin and
+    // the reference's piecewise Phi^ for the others); rb[m] is that bin for
+    // each representative, and a warp reads the particles of the bins between
+    // its representatives' extremes, a block those of its warps
+    int rb[kShell ? L : 1];
+    int beg = blockIdx.y * a.chunk, end = min(a.n, beg + a.chunk), w_lo = 0, w_hi = a.n;
+    if constexpr (kShell) {
+        int bmin = fa.shell_nbins, bmax = -1;
+#pragma unroll
+        for (int m = 0; m < L; ++m) {
+            rb[m] = hbin_of(fa.shell_edges, fa.shell_nbins, r[m] > 0.f ? fa.shell_r0 / r[m] : INFINITY);
+            bmin = min(bmin, rb[m]);
+            bmax = max(bmax, rb[m]);
+        }
+        if (!active) {
+            bmin = fa.shell_nbins;
+            bmax = -1;
+        }
+        bmin = __reduce_min_sync(0xffffffffu, bmin);
+        bmax = __reduce_max_sync(0xffffffffu, bmax);
+        w_lo = bmax < 0 ? 0 : fa.shell_first[bmin];
+        w_hi = bmax < 0 ? 0 : fa.shell_first[bmax + 1];
+        __shared__ int s_lo, s_hi;
+        if (tid == 0) {
+            s_lo = a.n;
+            s_hi = 0;
+        }
+        __syncthreads();
+        if ((tid & 31) == 0 && w_hi > w_lo) {
+            atomicMin(&s_lo, w_lo);
+            atomicMax(&s_hi, w_hi);
+        }
+        __syncthreads();
+        beg = s_lo;
+        end = s_hi;  // one split: the launcher runs the shell part unsplit
+    }
     const uint32_t uxb = (uint32_t)xb, uy = (uint32_t)yp, uz = (uint32_t)z;
 
     for (int t0 = beg; t0 < end; t0 += kThreads) {
@@ -310,14 +376,26 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
             double sn, cs;
             sincospi((double)(int32_t)qx * (1.0 / 2147483648.0), &sn, &cs);
             s_rot[tid] = make_float2((float)cs, (float)sn);
-            if constexpr (AMP == kAmpTable) s_h[tid] = a.radii[idx] * a.inv_ds;
+            if constexpr (kTab) s_h[tid] = a.radii[idx] * a.inv_ds;
             else if constexpr (AMP == kAmpExp2) {
                 const float h = a.radii[idx];
                 s_h[tid] = a.amp_scale * h * h;
             }
+            if constexpr (kShell) {
+                // the bin of sorted particle idx: the last b with first[b] <= idx
+                int lo = 0, hi = fa.shell_nbins;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (fa.shell_first[mid] <= idx) lo = mid;
+                    else hi = mid;
+                }
+                s_bin[tid] = lo;
+            }
         }
         __syncthreads();
-        const int cnt = min(kThreads, end - t0);
+        // this warp's particles of the tile (warp-uniform)
+        const int j0 = kShell ? max(0, w_lo - t0) : 0;
+        const int cnt = kShell ? min(min(kThreads, end - t0), w_hi - t0) : min(kThreads, end - t0);
 
         float2 acc[L][NP];
 #pragma unroll
@@ -326,11 +404,13 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
             for (int i = 0; i < NP; ++i) acc[m][i] = make_float2(0.f, 0.f);
 
 #pragma unroll 2
-        for (int j = 0; j < cnt; ++j) {
+        for (int j = j0; j < cnt; ++j) {
             const uint4 q = s_q[j];
             const float2 R = s_rot[j];
             float hv = 0.f;
             if constexpr (AMP != kAmpFactored) hv = s_h[j];
+            int pbin = 0;
+            if constexpr (kShell) pbin = s_bin[j];
             const float w = __uint_as_float(q.w);
             const uint32_t pyz = uy * q.y + uz * q.z;
             float sn, cs;
@@ -349,7 +429,7 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
                 float ur = cr, ui = ci;
                 if constexpr (AMP != kAmpFactored) {
                     float amp;
-                    if constexpr (AMP == kAmpTable) {
+                    if constexpr (kTab) {
                         // s / ds = r hv: nearest cell and offset (1.5 * 2^23 rounds)
                         const float tt = fmaf(r[m], hv, 12582912.0f);
                         const float fr = fmaf(r[m], hv, -(tt - 12582912.0f));
@@ -358,6 +438,7 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
                         const unsigned k = min((unsigned)(__float_as_int(tt) - 0x4B400000), (unsigned)a.table_n);
                         const float4 c = s_tab[k];
                         amp = fmaf(fmaf(fmaf(c.w, fr, c.z), fr, c.y), fr, c.x);
+                        if constexpr (kShell) amp = pbin == rb[m] ? amp : 0.f;
                     } else {
                         amp = exp2f(hv * r[m]);
                     }
@@ -421,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
 // fr = s/ds - k interpolating Phi^ (FP64, reference branch points) at the four
 // Chebyshev points of the cell.  Cells never straddle a branch point because
 // ds is chosen so that each branch point is a half-integer multiple of ds.
-__global__ void phi_table_kernel(int basis, double ds, int n, float4* out) {
+__global__ void phi_table_kernel(int basis, double ds, int n, float4* out, int kink) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k > n) return;
     if (k == n) {
@@ -432,7 +513,7 @@ __global__ void phi_table_kernel(int basis, double ds, int n, float4* out) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         x[i] = 0.5 * cospi((2 * i + 1) / 8.0);
-        f[i] = phi_fp64(basis, (k + x[i]) * ds);
+        f[i] = kink ? phi_kink_fp64(basis, (k + x[i]) * ds) : phi_fp64(basis, (k + x[i]) * ds);
     }
     // Newton divided differences, then expansion to monomials in fr.
     double d[4] = {f[0], f[1], f[2], f[3]};
@@ -538,6 +619,49 @@ SumKernel pick(int basis, int amp) {
 // for SPH, 0.24f for Wendland) sits at (K + 1/2) ds.
 double table_cell(int basis) { return basis == kSph ? (double)0.06f / 3.5 : (double)0.24f / 15.5; }
 
+// The folded lattice's representatives (xp, yp, z), xp < XP, yp < YP, z of
+// the lattice, sorted by |k|^2 and packed x | y << 10 | z << 20, in device
+// memory: built once per lattice shape and device and kept for the process.
+std::mutex g_reps_mu;
+std::map<std::tuple<int, int, int, int, double, double, double>, std::pair<uint32_t*, long long>> g_reps;
+
+int shell_representatives(const Lattice& lat, int xp_count, int yrows, const uint32_t** out, long long* count) {
+    if (xp_count > 1024 || yrows > 1024 || lat.z0 != 0 || lat.nz > 4096)
+        return set_error(kInvalidValue, "branch part: lattice too large for its representative list");
+    int dev = 0;
+    int st = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != kOk) return st;
+    const auto key = std::make_tuple(dev, xp_count, yrows, lat.nz, lat.kx, lat.ky, lat.kz);
+    std::lock_guard<std::mutex> lock(g_reps_mu);
+    auto it = g_reps.find(key);
+    if (it == g_reps.end()) {
+        std::vector<std::pair<double, uint32_t>> v;
+        v.reserve((size_t)xp_count * yrows * lat.nz);
+        for (int x = 0; x < xp_count; ++x)
+            for (int y = 0; y < yrows; ++y)
+                for (int z = 0; z < lat.nz; ++z) {
+                    const double kx = lat.kx * x, ky = lat.ky * y, kz = lat.kz * z;
+                    v.push_back({kx * kx + ky * ky + kz * kz, (uint32_t)x | ((uint32_t)y << 10) | ((uint32_t)z << 20)});
+                }
+        std::sort(v.begin(), v.end());
+        std::vector<uint32_t> packed(v.size());
+        for (size_t i = 0; i < v.size(); ++i) packed[i] = v[i].second;
+        uint32_t* d = nullptr;
+        st = check_cuda(cudaMalloc(&d, packed.size() * sizeof(uint32_t)), "cudaMalloc(representatives)");
+        if (st != kOk) return st;
+        st = check_cuda(cudaMemcpy(d, packed.data(), packed.size() * sizeof(uint32_t), cudaMemcpyHostToDevice),
+                        "representatives H2D");
+        if (st != kOk) {
+            cudaFree(d);
+            return st;
+        }
+        it = g_reps.emplace(key, std::make_pair(d, (long long)packed.size())).first;
+    }
+    *out = it->second.first;
+    *count = it->second.second;
+    return kOk;
+}
+
 }  // namespace
 
 int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
@@ -548,9 +672,14 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     if (req.n > 0 && req.particles == nullptr) return set_error(kInvalidValue, "dataset group has no device particles");
 
     const bool factored = req.radii == nullptr;
-    const int amp = factored ? kAmpFactored
-                    : (req.basis == kSph || req.basis == kWendland) ? kAmpTable
-                                                                      : kAmpExp2;
+    int amp = factored ? kAmpFactored
+              : (req.basis == kSph || req.basis == kWendland) ? kAmpTable
+                                                                : kAmpExp2;
+    if (req.kink) {
+        if (amp != kAmpTable || req.shell_nbins <= 0)
+            return set_error(kInvalidValue, "branch part needs SPH or Wendland with radii and h-bins");
+        amp = kAmpShell;
+    }
     const int L = lat.nx >= 8 ? 8 : 1;
     const int nxc = (lat.nx + L - 1) / L;
     const long long n_rest = (long long)lat.ny * lat.nz;
@@ -575,9 +704,16 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
             }
         }
     }
+    if (amp == kAmpShell && !fold_y) return set_error(kInvalidValue, "branch part needs a lattice holding x = 0, y = 0");
+    if (amp == kAmpShell) fold_l = 1;  // one representative per thread, sorted by |k|
     const int yrows = fold_y ? std::max(-lat.y0, lat.y0 + lat.ny - 1) + 1 : lat.ny;
     const int xpc = (xp_count + fold_l - 1) / fold_l;
-    const long long threads = fold ? (long long)xpc * yrows * lat.nz : (long long)nxc * n_rest;
+    const uint32_t* shell_reps = nullptr;
+    long long threads = fold ? (long long)xpc * yrows * lat.nz : (long long)nxc * n_rest;
+    if (amp == kAmpShell) {
+        int st_reps = shell_representatives(lat, xp_count, yrows, &shell_reps, &threads);
+        if (st_reps != kOk) return st_reps;
+    }
     if (threads > (1LL << 31) - 1) return set_error(kInvalidValue, "lattice too large");
     const long long blocks_f = (threads + kThreads - 1) / kThreads;
 
@@ -608,13 +744,14 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         }
         splits = best;
     }
+    if (amp == kAmpShell) splits = 1;  // each block reads a few h-bins only
     long long chunk = req.n > 0 ? ((req.n + splits - 1) / splits + kThreads - 1) / kThreads * kThreads : kThreads;
     splits = req.n > 0 ? (req.n + chunk - 1) / chunk : 1;
 
     // Table size: cells up to the largest s = |k|max * hmax (when known).
     int table_n = 0;
     double ds = 0.0;
-    if (amp == kAmpTable) {
+    if (amp == kAmpTable || amp == kAmpShell) {
         ds = table_cell(req.basis);
         const double kx = std::fabs(lat.kx) * std::max(std::abs(lat.x0), std::abs(lat.x0 + lat.nx - 1));
         const double ky = std::fabs(lat.ky) * std::max(std::abs(lat.y0), std::abs(lat.y0 + lat.ny - 1));
@@ -625,11 +762,13 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         // and the zero cell stands in for it.
         table_n = (int)std::min<double>(kMaxTable, std::ceil(smax / ds) + 2.0);
         table_n = std::max(table_n, 1);
+        // the branch part ends at the branch point, (K + 1/2) ds: cells 0 .. K
+        if (req.kink) table_n = std::min(table_n, (int)std::llround(phi_branch_point(req.basis) / ds - 0.5) + 1);
     }
 
     const size_t plane = fold ? (size_t)lat.nx * n_rest : (size_t)nxc * L * n_rest;
     const size_t part_bytes = (plane * splits * sizeof(float2) + 255) / 256 * 256;
-    const size_t table_cells = amp == kAmpTable ? (size_t)table_n + 1 : 0;
+    const size_t table_cells = (amp == kAmpTable || amp == kAmpShell) ? (size_t)table_n + 1 : 0;
     const size_t table_bytes = (table_cells * sizeof(float4) + 255) / 256 * 256;
     // folded form: the running FP64 sums, 2 FY pairs per representative
     const size_t sums_bytes =
@@ -651,9 +790,9 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
     a.inv_ds = ds > 0 ? (float)(1.0 / ds) : 0.f;
     a.amp_scale = req.basis == kGaussian ? kPiLog2e : -kPiLog2e;
 
-    if (amp == kAmpTable) {
+    if (amp == kAmpTable || amp == kAmpShell) {
         phi_table_kernel<<<(table_n + 128) / 128, 128, 0, req.stream>>>(req.basis, ds, table_n,
-                                                                         const_cast<float4*>(a.table));
+                                                                         const_cast<float4*>(a.table), req.kink);
         count_launch();
     }
 
@@ -665,10 +804,17 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         fa.yrows = yrows;
         fa.plane = plane;
         fa.sums = reinterpret_cast<double2*>(static_cast<char*>(ws.ptr) + part_bytes + table_bytes);
-        FoldKernel k = !fold_y        ? pick_fold<8, 1>(amp)
-                       : fold_l == 4 ? pick_fold<4, 2>(amp)
-                       : fold_l == 5 ? pick_fold<5, 2>(amp)
-                                     : pick_fold<6, 2>(amp);
+        fa.shell_nbins = req.kink ? req.shell_nbins : 0;
+        fa.shell_edges = req.shell_edges;
+        fa.shell_first = req.shell_first;
+        fa.shell_r0 = (float)phi_branch_point(req.basis);
+        fa.shell_reps = shell_reps;
+        fa.shell_count = (int)threads;
+        FoldKernel k = amp == kAmpShell ? fold_sum_kernel<1, 2, kAmpShell>
+                       : !fold_y      ? pick_fold<8, 1>(amp)
+                       : fold_l == 4  ? pick_fold<4, 2>(amp)
+                       : fold_l == 5  ? pick_fold<5, 2>(amp)
+                                      : pick_fold<6, 2>(amp);
         if (dyn_smem > 48 * 1024) {
             st = check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem),
                             "cudaFuncSetAttribute");
@@ -843,7 +989,7 @@ extern "C" int vis_fourier_slice_sum_noalloc(const Constraint* d_constraints, co
     a.amp_scale = basis == kGaussian ? kPiLog2e : -kPiLog2e;
 
     if (amp == kAmpTable) {
-        phi_table_kernel<<<(table_n + 128) / 128, 128, 0, stream>>>(basis, ds, table_n, const_cast<float4*>(a.table));
+        phi_table_kernel<<<(table_n + 128) / 128, 128, 0, stream>>>(basis, ds, table_n, const_cast<float4*>(a.table), 0);
         count_launch();
     }
     SumKernel k = (L == 8) ? pick<8>(basis, amp) : pick<1>(basis, amp);

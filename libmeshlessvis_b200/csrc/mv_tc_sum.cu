@@ -25,11 +25,13 @@
 // stages (a chain of flush_stages x 12 MMAs; the tensor core's FP32
 // accumulation loses accuracy with chain length: 1.6e-6 rel-L2 at 4 stages,
 // 2.4e-6 at 8, 4.1e-6 at 16) the MMA pauses while the flush warps add the
-// accumulator into an FP32 total in the other 256 TMEM columns.  Every
-// kDumpFlushes chains, and at the end of the particle range, the total goes
-// to an FP64 accumulator in global memory (RED.ADD.F64, laid out [c][Re, Im][row]
-// so a warp's rows are contiguous), which a finalize kernel converts to the
-// float2 spectrum.
+// accumulator into an FP32 total in the other 256 TMEM columns.  At the end
+// of its particle range (at most kMaxItemChains chains) a work item stores its
+// total once, with plain coalesced stores, into its own slot of global memory
+// ([column][row]: a warp's rows are contiguous).  No atomics: tc_reduce_kernel
+// then sums every element's slots over particle chunks and jobs (groups,
+// h-bins) in FP64, in a fixed order, and adds the result to the float2
+// spectrum, so results are bitwise reproducible.
 //
 // The Nyquist plane c = Kz/2 is the same kind of GEMM with the axes
 // exchanged: rows b with the fixed frequency Kz/2 on z, columns a on x (two
@@ -119,9 +121,11 @@ constexpr int kLoaderWarp = 1 + kFlushWarps + kProducerWarps;
 constexpr int kThreads = 32 * (kLoaderWarp + 1);
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColTotal = 256;  // FP32 total: columns [256, 256 + accumulator columns)
-constexpr int kDumpFlushes = 16;  // chain partials summed in FP32 before an FP64 dump
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
-constexpr float kInvProductScale = 1.f / (4096.f * 4096.f);  // 2^-24
+constexpr double kInvProductScale = 1.0 / (4096.0 * 4096.0);  // 2^-24
+// An item sums at most this many accumulation chains in its FP32 total
+// (random-walk rounding of about 2^-24 sqrt(64) of the total).
+constexpr int kMaxItemChains = 64;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 // After a wait has run out, a CTA idles this long before it releases TMEM and
 // exits, so bulk copies it issued (which complete within microseconds) have
@@ -210,6 +214,7 @@ struct TcItem {
     int period;                  // h-binned job: frequency columns per Chebyshev block (else 0)
     const unsigned char* bimg;   // this CTA's B-operand images of the item's n-tile (one per block), or null
     int img_stride, img_bytes;   // bytes between images; bytes of one image (512 bnc)
+    float* slot;                 // this CTA's part of the item's result tile: [column / 4][128 rows][column % 4]
 };
 
 template <int MODE>
@@ -240,6 +245,7 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.bimg = r.job->bimg ? r.job->bimg + (size_t)(r.n_tile * Shape<MODE>::kCtas + rank) * r.job->n_blocks *
                                              (size_t)r.img_stride
                          : nullptr;
+    r.slot = r.job->slots + (size_t)v.y * r.job->slot_stride + (size_t)rank * kM * 2 * r.job->nc_tile;
     return r;
 }
 
@@ -591,41 +597,6 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
     else b_chain<false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, make_float2(1.f, 1.f), RHO);
 }
 
-// The dump of an h-binned job's 32 total columns cc .. cc + 31 for one row
-// (out of line: the Chebyshev bookkeeping stays out of the kernel's register
-// budget).  Column c is Chebyshev block q = c / period at frequency column
-// c % period; its value is weighted by the block's coefficient at |k|^2 =
-// a^2 + b^2 + c^2 and added into that frequency column of the accumulator.
-__device__ __noinline__ void dump_binned(const TcItem& I, const float* tt, int cc, int ncols, int half_cols, int rho,
-                                         bool in_rows, size_t mk, double* acc, double dump_scale) {
-    if (!in_rows) return;
-    const int a_f = rho / I.job->ky + I.a_base, b_f = rho % I.job->ky + I.b_base;
-    const int ab2 = a_f * a_f + b_f * b_f;
-    const float* coef = I.job->coef;
-    const int stride = I.job->coef_stride;
-    // in batches of 8 columns: every coefficient load of a batch is issued
-    // before the first is used, so their L2 latencies overlap
-#pragma unroll 1
-    for (int i0 = 0; i0 < 32; i0 += 8) {
-        float w[8];
-        int dst[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int n = min(cc + i0 + i, ncols - 1);  // columns past ncols: loaded, not added
-            const int h = n / half_cols, nn = n - h * half_cols;
-            const int im = nn >= I.bnc ? 1 : 0;
-            const int c = I.c0 + h * I.bnc + nn - im * I.bnc;
-            const int q = c / I.period, cf = c - q * I.period, cfreq = cf + I.c_base;
-            w[i] = __ldg(coef + (size_t)q * stride + ab2 + cfreq * cfreq);
-            dst[i] = 2 * cf + im;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-            if (cc + i0 + i < ncols)
-                atomicAdd(acc + (size_t)dst[i] * mk + rho, (double)tt[i0 + i] * dump_scale * (double)w[i]);
-    }
-}
-
 // Persistent: CTA (or CTA pair) b walks items b, b + grid, ... of the
 // longest-first item list.  Every role walks the same items in the same
 // order, and the pipeline's stage and chain counters (hence mbarrier phases
@@ -783,16 +754,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         int C = 0;
         for (int it = unit; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += n_units) {
             const TcItem I = tc_item<MODE>(a, it, rank);
-            const size_t mk = (size_t)I.job->kx * I.job->ky;
-            double* acc = I.job->acc;
-            // the accumulator and the total hold 2^24 x the sum (units of the
-            // operand scale); the exact 2^-24 is applied with W at the dump
-            const double dump_scale = I.job->wmax * (double)kInvProductScale;
-            const int rho = I.row0 + row;
-            const bool in_rows = (size_t)rho < mk;  // rows of a partial last m-tile are not dumped
-            const int c0 = I.c0;
             const int ncols = 2 * I.nc;
-            const int half_cols = 2 * I.bnc;  // columns from one CTA's B rows (all of them unless kPair)
+            float* slot = I.slot + row * 4;  // columns n..n+3 (n % 4 == 0) at slot[(n / 4) * 512]: quads of rows
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
                 const int b = k % kBufs, u = k / kBufs;
@@ -801,14 +764,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, a.wait_limit_ns, 4))) break;
                 tc_fence_after();
                 tmem_wait_st();  // the previous flush's stores of the total
-                // chain partials are summed in FP32 for kDumpFlushes chains, then
-                // dumped into the FP64 accumulator (and at the item's end)
-                const bool first = (kk % kDumpFlushes) == 0;
-                const bool dump = (kk % kDumpFlushes) == kDumpFlushes - 1 || kk == I.n_chunks - 1;
+                // the item's chain partials are summed into an FP32 total in
+                // TMEM; the last chain's sum goes to the item's slot instead
+                const bool first = kk == 0;
+                const bool last = kk == I.n_chunks - 1;
                 // 32 columns per round trip.  ncols is a multiple of 16, so the
                 // last trip may carry 16 columns past ncols: they stay inside
-                // the accumulator and total regions, are never dumped, and the
-                // total's copy is overwritten by the next item's first flush.
+                // the accumulator and total regions and are never stored.
 #pragma unroll 1
                 for (int cc = 0; cc < ncols; cc += 32) {
                     float tt[32];
@@ -827,7 +789,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                             tt[i + 1] = t2.y;
                         }
                     }
-                    tmem_st32(lane_base + kColTotal + cc, tt);
+                    if (!last) {
+                        tmem_st32(lane_base + kColTotal + cc, tt);
+                    } else {
+                        // ncols is a multiple of 16: whole float4 groups are in or out;
+                        // a warp's 32 rows write 512 contiguous bytes per group
+#pragma unroll
+                        for (int i = 0; i < 32; i += 4)
+                            if (cc + i < ncols)
+                                *reinterpret_cast<float4*>(slot + (size_t)(cc + i) * kM) =
+                                    make_float4(tt[i], tt[i + 1], tt[i + 2], tt[i + 3]);
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -837,34 +809,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     // own warps arrive locally
                     if (rank == 0) mbar_arrive(&acc_empty[b]);
                     else mbar_arrive_leader(&acc_empty[b]);
-                }
-                if (dump) {
-                    // the total is read back from its own TMEM columns, which
-                    // the MMAs never write: the dump overlaps the next chain
-                    tmem_wait_st();
-#pragma unroll 1
-                    for (int cc = 0; cc < ncols; cc += 32) {
-                        float tt[32];
-                        tmem_ld32(lane_base + kColTotal + cc, tt);
-                        tmem_wait_ld();
-                        if (I.period == 0) {
-                            // FP64 accumulator [c][Re, Im][row]: a warp's 32 rows
-                            // are contiguous.  Column n: CTA h = n / half_cols's B
-                            // rows, Re then Im of its bnc c values.
-#pragma unroll
-                            for (int i = 0; i < 32; ++i) {
-                                const int n = cc + i;
-                                if (n < ncols && in_rows) {
-                                    const int h = n / half_cols, nn = n - h * half_cols;
-                                    const int im = nn >= I.bnc ? 1 : 0;
-                                    const int c = c0 + h * I.bnc + nn - im * I.bnc;
-                                    atomicAdd(acc + (size_t)(2 * c + im) * mk + rho, (double)tt[i] * dump_scale);
-                                }
-                            }
-                        } else {
-                            dump_binned(I, tt, cc, ncols, half_cols, rho, in_rows, mk, acc, dump_scale);
-                        }
-                    }
                 }
             }
             C += I.n_chunks;
@@ -1155,24 +1099,15 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
 //   Phi^(|k| h_j) ~= sum_q c_q(|k|) T_q(t_j),  t_j = (2 h_j - lo - hi) / (hi - lo),
 //   c_q(|k|) = (2 / P) sum_p Phi^(|k| h_p) T_q(x_p)  (c_0 halved),
 // so the bin's sum is, per q, a separable sum with B-side weights T_q(t_j)
-// (one job per bin whose columns are the q blocks), and c_q(|k|) multiplies
-// the q-th block when it is dumped.  The bins and orders are chosen on the
-// host (hbin_plan) so the interpolation error stays near 1e-6 of the sum.
-
-// Bin of radius h among nb bins with edges e[0..nb]: the largest i with
-// e[i] <= h, clamped to [0, nb) -- the rule hbin_fine_index applies to the
-// fine edges at registration, whose counts the bins' capacities come from.
-__device__ __forceinline__ int hbin_of(const float* e, int nb, float h) {
-    if (nb <= 1 || !(h >= e[1])) return 0;
-    if (h >= e[nb - 1]) return nb - 1;
-    int lo = 0, hi = nb;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (e[mid] <= h) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
+// (one job per bin whose columns are the q blocks), and the reduction
+// multiplies block q by c_q(|k|).  The reference's Phi^ switches from a
+// quadratic fit to the closed form C at a branch point r0 with a jump in
+// slope, which no polynomial in h follows; at frequency k that kink lies in
+// the one bin holding r0 / |k|.  For that bin the coefficients are C's, and
+// the plain form adds Phi^ - C (zero from r0 on) for the bin's particles at
+// that k, over the particles sorted by bin (about 0.5% of the plain form's
+// work on the SPH-like set).  The bins and orders are chosen on the host
+// (hbin_plan) so the interpolation error stays near 1e-6 of the sum.
 
 struct TcBinnedPrepArgs {
     const float4* particles;
@@ -1186,6 +1121,9 @@ struct TcBinnedPrepArgs {
     int* cursors;          // nbins, zero at launch
     uint8_t* out;          // the group's blocks, bin by bin
     uint8_t* out_nyq;      // the same with x and z exchanged, or null
+    const int* first;      // nbins + 1: the bins' first particles in sorted order
+    float4* sorted;        // particles sorted by bin (for the branch part)
+    float* sorted_radii;
     int* error_flag;
 };
 
@@ -1206,6 +1144,8 @@ __global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
     const float4 sp = p.spans[b];
     const float t = sp.y > sp.x ? (2.f * h - sp.x - sp.y) / (sp.y - sp.x) : 0.f;
     const float4 q = p.particles[j];
+    p.sorted[p.first[b] + slot] = q;
+    p.sorted_radii[p.first[b] + slot] = h;
     const uint32_t qx = fixed_turns(p.step * (double)q.x);
     const uint32_t qy = fixed_turns(p.step * (double)q.y);
     const uint32_t qz = fixed_turns(p.step * (double)q.z);
@@ -1231,15 +1171,23 @@ struct TcCoefArgs {
     int basis;
     double step;
     int nbins;
-    int nsq;               // entries per (bin, q): |k|^2 / step^2 = 0 .. nsq - 1
-    const int4* bins;      // (first block, capacity, coef offset, order)
+    int nsq;               // |k|^2 / step^2 = 0 .. nsq - 1
+    int total_q;           // the group's Chebyshev blocks over all bins
+    const int4* bins;      // (first block, capacity, first Chebyshev block, order)
     const float4* spans;   // (lo, hi, ...)
+    const float* edges;    // the bins' classification edges
+    float r0;              // the basis's branch point
     float* coef;
 };
 
 // Chebyshev coefficients c_q(|k|) of h -> Phi^(|k| h) on each bin, for every
-// integer |k|^2 / step^2 of the lattice, in FP64 (the reference's Phi^
-// formulas), stored as floats: coef[offset + q * nsq + n2].
+// integer |k|^2 / step^2 of the lattice, in FP64, stored as floats:
+// coef[n2 * total_q + q_offset(bin) + q] (one |k|^2's coefficients together,
+// as the reduction reads them).  Phi^ is smooth on a bin unless the bin holds
+// r0 / |k| (the reference's branch point, where its slope jumps): for that one
+// bin the smooth closed form is interpolated instead (phi_smooth_fp64), and
+// the plain form adds the rest for the bin's particles at that k
+// (kAmpShell, mv_sum.cu).  Both sides find the bin from the same float |k|.
 __global__ void tc_coef_kernel(TcCoefArgs c) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)c.nbins * c.nsq) return;
@@ -1248,19 +1196,22 @@ __global__ void tc_coef_kernel(TcCoefArgs c) {
     const float4 sp = c.spans[b];
     const int order = bin.w;
     const double k = c.step * sqrt((double)n2);
+    const float kf = (float)sqrt(c.step * c.step * (double)n2);
+    const bool shell = hbin_of(c.edges, c.nbins, kf > 0.f ? c.r0 / kf : INFINITY) == b;
     const double mid = 0.5 * ((double)sp.x + (double)sp.y), half = 0.5 * ((double)sp.y - (double)sp.x);
     constexpr int kMaxOrder = 16;
     double f[kMaxOrder], x[kMaxOrder];
     for (int p = 0; p < order && p < kMaxOrder; ++p) {
         x[p] = cospi((2.0 * p + 1.0) / (2.0 * order));
-        f[p] = phi_fp64(c.basis, k * (mid + half * x[p]));
+        const double r = k * (mid + half * x[p]);
+        f[p] = shell ? phi_smooth_fp64(c.basis, r) : phi_fp64(c.basis, r);
     }
     for (int q = 0; q < order && q < kMaxOrder; ++q) {
         double acc = 0.0;
         for (int p = 0; p < order; ++p) acc += f[p] * cospi(q * (2.0 * p + 1.0) / (2.0 * order));
         acc *= 2.0 / order;
         if (q == 0) acc *= 0.5;
-        c.coef[(size_t)bin.z + (size_t)q * c.nsq + n2] = (float)acc;
+        c.coef[(size_t)n2 * c.total_q + bin.z + q] = (float)acc;
     }
 }
 
@@ -1269,24 +1220,34 @@ __global__ void tc_coef_kernel(TcCoefArgs c) {
 // values of 2 particles, exactly as a producer warp would into the stage
 // buffer.  Each image is written once and copied by the tensor kernel's loader
 // for every m-tile of the job.
+// All jobs' images in one launch: CTA i makes image i of the concatenation,
+// [job with images][n_tile][CTA half][block], the job found by binary search
+// over the image offsets (img_first[k]: first image of the k-th such job).
 struct TcImageArgs {
-    const unsigned char* blocks;
-    unsigned char* bimg;
-    int n_blocks, img_stride;
-    int ctas, nc_tile, lz_tc, c_base, period;
-    bool gauss;
+    const TcJob* jobs;
+    const int* img_jobs;          // the jobs that have images
+    const long long* img_first;   // n_img_jobs + 1 offsets
+    int n_img_jobs;
 };
 
 __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
-    const long long img = blockIdx.x;  // (n_tile * ctas + half) * n_blocks + block
-    const int block = (int)(img % g.n_blocks);
-    const int nh = (int)(img / g.n_blocks);
-    const int half = nh % g.ctas, n_tile = nh / g.ctas;
-    const int c0 = n_tile * g.nc_tile;
-    const int bnc = min(g.nc_tile, g.lz_tc - c0) / g.ctas;
+    const long long i = blockIdx.x;
+    int lo = 0, hi = g.n_img_jobs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (g.img_first[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    const TcJob& J = g.jobs[g.img_jobs[lo]];
+    const long long img = i - g.img_first[lo];  // (n_tile * ctas + half) * n_blocks + block
+    const int block = (int)(img % J.n_blocks);
+    const int nh = (int)(img / J.n_blocks);
+    const int half = nh % J.ctas, n_tile = nh / J.ctas;
+    const int c0 = n_tile * J.nc_tile;
+    const int bnc = min(J.nc_tile, J.lz_tc - c0) / J.ctas;
     const int pp = threadIdx.x & 15, chunk = threadIdx.x >> 4;
     if (chunk * 8 >= bnc) return;
-    const unsigned char* blk = g.blocks + (size_t)block * kBlockBytes;
+    const unsigned char* blk = J.blocks + (size_t)block * kBlockBytes;
     const uint2 zq = *reinterpret_cast<const uint2*>(blk + kOffQz + 8 * pp);
     const uint2 gq = *reinterpret_cast<const uint2*>(blk + kOffGam + 8 * pp);
     const uint2 rq = *reinterpret_cast<const uint2*>(blk + kOffRho2 + 8 * pp);
@@ -1295,20 +1256,102 @@ __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
     const float pgam[2] = {__uint_as_float(gq.x), __uint_as_float(gq.y)};
     const float2 RX = make_float2(r.x, r.z), RY = make_float2(r.y, r.w);
     const float2 NRY = make_float2(-RY.x, -RY.y);
-    const float2 RHO = g.gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
-    uint8_t* out = g.bimg + (size_t)img * g.img_stride;
-    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, g.c_base, g.period, pqz, pgam, g.gauss, RX, RY, NRY,
+    const bool gauss = J.gauss != 0;
+    const float2 RHO = gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
+    uint8_t* out = const_cast<uint8_t*>(J.bimg) + (size_t)img * J.img_stride;
+    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, J.c_base, J.period, pqz, pgam, gauss, RX, RY, NRY,
            RHO);
 }
 
-// acc (FP64) -> float2 spectrum planes c in [0, lz_tc): times the per-frequency
-// Phi^ factor (groups whose Phi^ factors out) and the scale, written or added.
-// nyquist: the plane c = lz_tc alone, from the transposed jobs' accumulator
-// [column][Re, Im][row]: for a >= 0, column a + Kx/2 and row b + Ky/2; for a <
-// 0 the conjugate of column -a - 1 (frequency -a) at row Ky/2 - 1 - b
-// (frequency -b).
-struct TcFinalizeArgs {
-    const double* acc;
+// What the reduction needs of a job, gathered into shared memory once per
+// block (the job table's other fields are not read).
+struct ReduceJob {
+    const float* slots;
+    const int4* colmap;
+    const float* coef;  // null unless h-binned
+    double scale;       // W x 2^-24
+    int slot_stride, n_splits, n_mtiles, n_ntiles;
+    int rank_stride;    // floats between the CTAs' parts of a slot: 128 * 2 nc_tile
+    int mrows_log2;     // 7 (one CTA) or 8 (CTA pair)
+    int period, blocks, coef_stride;
+};
+
+__device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
+    ReduceJob r;
+    r.slots = J.slots;
+    r.colmap = J.colmap;
+    r.coef = J.period > 0 ? J.coef : nullptr;
+    r.scale = J.wmax * kInvProductScale;
+    r.slot_stride = J.slot_stride;
+    r.n_splits = J.n_splits;
+    r.n_mtiles = J.n_mtiles;
+    r.n_ntiles = J.n_ntiles;
+    r.rank_stride = kM * 2 * J.nc_tile;
+    r.mrows_log2 = J.ctas == 2 ? 8 : 7;
+    r.period = J.period;
+    r.blocks = J.period > 0 ? J.lz_tc / J.period : 1;
+    r.coef_stride = J.coef_stride;
+    return r;
+}
+
+// Adds one job's contribution at lattice row rho (within the job's rows) and
+// the kC consecutive frequency columns c0 .. c0 + kC - 1 (c_idx, before the
+// Chebyshev blocks of an h-binned job; they share one n-tile and one CTA half,
+// as n-tiles and halves hold multiples of 8 columns): the FP32 tiles of all
+// its particle chunks summed in FP64, each h-binned block weighted by its
+// coefficient at |k|^2 = n2[i] step^2, times W 2^-24.
+constexpr int kReduceC = 4;
+__device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, const int* n2, int nc, double* sr,
+                                           double* si, double sign_im) {
+    const int m_tile = rho >> J.mrows_log2, within = rho - (m_tile << J.mrows_log2);
+    const int rank = within >> 7, rl = within & (kM - 1);
+    // slot layout [column / 4][128 rows][column % 4]: column n of row rl at
+    // (n / 4) * 512 + rl * 4 + n % 4
+    const float* row = J.slots + (size_t)rank * J.rank_stride + rl * 4;
+    for (int q = 0; q < J.blocks; ++q) {
+        const int4 m = __ldg(J.colmap + q * J.period + c0);  // the same for a warp's rows
+        double tr[kReduceC] = {}, ti[kReduceC] = {};
+        for (int ks = 0; ks < J.n_splits; ++ks) {
+            const size_t li = ((size_t)ks * J.n_mtiles + m_tile) * J.n_ntiles + m.x;
+            const float* v = row + li * J.slot_stride;
+            if (nc == kReduceC) {
+                // four columns in one load (m.y, m.z are multiples of 4); a warp's
+                // rows read 512 contiguous bytes
+                const float4 re = __ldg(reinterpret_cast<const float4*>(v + (size_t)m.y * kM));
+                const float4 im = __ldg(reinterpret_cast<const float4*>(v + (size_t)m.z * kM));
+                tr[0] += re.x; tr[1] += re.y; tr[2] += re.z; tr[3] += re.w;
+                ti[0] += im.x; ti[1] += im.y; ti[2] += im.z; ti[3] += im.w;
+            } else {
+                tr[0] += (double)__ldg(v + (size_t)(m.y & ~3) * kM + (m.y & 3));
+                ti[0] += (double)__ldg(v + (size_t)(m.z & ~3) * kM + (m.z & 3));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kReduceC; ++i) {
+            if (i < nc) {
+                const double w = J.coef ? (double)__ldg(J.coef + (size_t)n2[i] * J.coef_stride + q) * J.scale : J.scale;
+                sr[i] = fma(w, tr[i], sr[i]);
+                si[i] = fma(w * sign_im, ti[i], si[i]);
+            }
+        }
+    }
+}
+
+// The jobs of one output class (same spectrum, same per-frequency factor)
+// -> its float2 spectrum, added: planes c in [0, lz_tc), or (nyquist) the
+// plane c = lz_tc from the transposed jobs: for a >= 0 the a >= 0 jobs at row
+// b_idx and column a; for a < 0 the conjugate of the a < 0 jobs at row
+// Ky - 1 - b_idx (frequency -b) and column -a - 1 (frequency -a).  Times the
+// factored Phi^(|k| h) in FP64 and the scale.  Thread: kReduceC consecutive
+// planes of one row (nyquist: one element), rows fastest (the slots' reads
+// are coalesced); the block gathers the class's job descriptors in shared
+// memory first.
+struct TcReduceArgs {
+    const TcJob* jobs;
+    const int* list;      // planes: the class's jobs; nyquist: its a >= 0 jobs
+    int n_list;
+    const int* list_neg;  // nyquist: its a < 0 jobs
+    int n_neg;
     int kx, ky, lz_tc, lz_out;
     double step;
     int basis;
@@ -1316,49 +1359,91 @@ struct TcFinalizeArgs {
     bool factored;
     double scale;
     float2* out;
-    bool accumulate;
     bool nyquist;
 };
 
-__global__ void tc_finalize_kernel(TcFinalizeArgs f) {
+__global__ void __launch_bounds__(256) tc_reduce_kernel(TcReduceArgs f) {
+    extern __shared__ ReduceJob s_jobs[];  // n_list (+ n_neg) descriptors
+    const int n_all = f.n_list + (f.nyquist ? f.n_neg : 0);
+    for (int i = threadIdx.x; i < n_all; i += blockDim.x)
+        s_jobs[i] = reduce_job(f.jobs[i < f.n_list ? f.list[i] : f.list_neg[i - f.n_list]]);
+    __syncthreads();
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int planes = f.nyquist ? 1 : f.lz_tc;
-    const long long count = (long long)f.kx * f.ky * planes;
-    if (q >= count) return;
-    const int c = f.nyquist ? f.lz_tc : (int)(q % f.lz_tc);
-    const long long rho = q / planes;
-    const int b = (int)(rho % f.ky) - f.ky / 2;
-    const int a = (int)(rho / f.ky) - f.kx / 2;
-    double factor = f.scale;
-    if (f.factored) {
-        const double k = f.step * sqrt((double)a * a + (double)b * b + (double)c * c);
-        factor *= phi_fp64(f.basis, k * f.h);
-    }
-    size_t i_re, i_im;
-    double conj = 1.0;
-    if (f.nyquist) {
-        const int a_idx = (int)(rho / f.ky), b_idx = (int)(rho % f.ky);
-        if (a >= 0) {
-            i_re = (size_t)(2 * a_idx) * f.ky + b_idx;
-        } else {
-            i_re = (size_t)(2 * (-a - 1)) * f.ky + (f.ky - 1 - b_idx);
-            conj = -1.0;
-        }
-        i_im = i_re + f.ky;
+    const long long rows = (long long)f.kx * f.ky;
+    const int groups = f.nyquist ? 1 : f.lz_tc / kReduceC;  // lz_tc is a multiple of 8
+    if (q >= rows * groups) return;
+    const int rho = (int)(q % rows);
+    const int a_idx = rho / f.ky, b_idx = rho % f.ky;
+    const int a = a_idx - f.kx / 2, b = b_idx - f.ky / 2;
+    const int c0 = f.nyquist ? f.lz_tc : (int)(q / rows) * kReduceC;
+    const int nc = f.nyquist ? 1 : kReduceC;
+    int n2[kReduceC];
+#pragma unroll
+    for (int i = 0; i < kReduceC; ++i) n2[i] = a * a + b * b + (c0 + i) * (c0 + i);
+    double sr[kReduceC] = {}, si[kReduceC] = {};
+    if (!f.nyquist) {
+        for (int j = 0; j < f.n_list; ++j) reduce_add(s_jobs[j], rho, c0, n2, nc, sr, si, 1.0);
+    } else if (a >= 0) {
+        for (int j = 0; j < f.n_list; ++j) reduce_add(s_jobs[j], b_idx, a, n2, 1, sr, si, 1.0);
     } else {
-        // accumulator layout [c][Re, Im][row]
-        const size_t mk = (size_t)f.kx * f.ky;
-        i_re = (size_t)(2 * c) * mk + rho;
-        i_im = i_re + mk;
+        for (int j = 0; j < f.n_neg; ++j)
+            reduce_add(s_jobs[f.n_list + j], f.ky - 1 - b_idx, -a - 1, n2, 1, sr, si, -1.0);
     }
-    const float re = (float)(f.acc[i_re] * factor);
-    const float im = (float)(f.acc[i_im] * factor * conj);
-    const size_t idx = (size_t)rho * f.lz_out + c;
-    if (f.accumulate) {
+#pragma unroll
+    for (int i = 0; i < kReduceC; ++i) {
+        if (i >= nc) break;
+        double factor = f.scale;
+        if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[i]) * f.h);
+        const size_t idx = (size_t)rho * f.lz_out + c0 + i;
         const float2 o = f.out[idx];
-        f.out[idx] = make_float2(o.x + re, o.y + im);
-    } else {
-        f.out[idx] = make_float2(re, im);
+        f.out[idx] = make_float2(o.x + (float)(sr[i] * factor), o.y + (float)(si[i] * factor));
+    }
+}
+
+// The planes c < lz_tc of one output class, with the job list split over
+// warps: a block takes 32 rows (lanes) x kReduceC planes, warp w sums jobs w,
+// w + 8, ..., and the eight partial sums are added in warp order (a fixed
+// order: the result does not depend on timing), so eight independent load
+// chains per element hide the slots' latency.
+constexpr int kReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kReduceWarps) tc_reduce_planes_kernel(TcReduceArgs f) {
+    extern __shared__ __align__(16) unsigned char s_raw[];  // n_list descriptors, then the partial sums
+    ReduceJob* s_jobs = reinterpret_cast<ReduceJob*>(s_raw);
+    for (int i = threadIdx.x; i < f.n_list; i += blockDim.x) s_jobs[i] = reduce_job(f.jobs[f.list[i]]);
+    // [warp][lane][kReduceC], 16-byte aligned after the descriptors
+    double2* s_part = reinterpret_cast<double2*>(s_raw + (((size_t)f.n_list * sizeof(ReduceJob) + 15) & ~(size_t)15));
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long rows = (long long)f.kx * f.ky;
+    const long long row_blocks = (rows + 31) / 32;
+    const int rho = (int)((blockIdx.x % row_blocks) * 32 + lane);
+    const int c0 = (int)(blockIdx.x / row_blocks) * kReduceC;
+    const bool active = rho < rows;
+    const int rr = active ? rho : 0;
+    const int a = rr / f.ky - f.kx / 2, b = rr % f.ky - f.ky / 2;
+    int n2[kReduceC];
+#pragma unroll
+    for (int i = 0; i < kReduceC; ++i) n2[i] = a * a + b * b + (c0 + i) * (c0 + i);
+    double sr[kReduceC] = {}, si[kReduceC] = {};
+    if (active)
+        for (int j = warp; j < f.n_list; j += kReduceWarps) reduce_add(s_jobs[j], rho, c0, n2, kReduceC, sr, si, 1.0);
+#pragma unroll
+    for (int i = 0; i < kReduceC; ++i) s_part[(warp * 32 + lane) * kReduceC + i] = make_double2(sr[i], si[i]);
+    __syncthreads();
+    if (warp != 0 || !active) return;
+#pragma unroll
+    for (int i = 0; i < kReduceC; ++i) {
+        double tr = 0.0, ti = 0.0;
+        for (int w = 0; w < kReduceWarps; ++w) {
+            const double2 v = s_part[(w * 32 + lane) * kReduceC + i];
+            tr += v.x;
+            ti += v.y;
+        }
+        double factor = f.scale;
+        if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[i]) * f.h);
+        const size_t idx = (size_t)rho * f.lz_out + c0 + i;
+        const float2 o = f.out[idx];
+        f.out[idx] = make_float2(o.x + (float)(tr * factor), o.y + (float)(ti * factor));
     }
 }
 
@@ -1453,14 +1538,10 @@ namespace {
 // bins needing more than kHBinMaxOrder nodes are not formed.
 constexpr double kHBinTau = 3e-5;
 constexpr int kHBinMaxOrder = 12;
-// The reference's Phi^ switches from a quadratic fit to the closed form at a
-// branch point r0 (0.06 SPH, 0.24 Wendland; fourier_transform.cu:33, :50),
-// where its slope jumps by 0.4% (SPH) and 1.3% (Wendland) of Phi^(0).  No
-// polynomial in h follows that kink, so a bin whose |k| h reaches r0 on the
-// lattice is kept at most kHBinKinkWidth wide (hi / lo - 1): the kink then
-// costs a few 1e-7 of the sum (CPU models of the scheme against the oracle's
-// FP64 Phi^: C2's set 6e-8, uniform sets with h in [0.01, 0.05] up to 7e-7).
-constexpr double kHBinKinkWidth = 0.05;
+// The bins interpolate the closed form C only (the branch's part is summed
+// apart, see tc_coef_kernel), which is smooth: CPU models of the scheme
+// against the oracle's FP64 Phi^ give 4e-8 rel-L2 on C2's set and up to 7e-7
+// on uniform sets with h in [0.01, 0.05].
 
 double hbin_order_limit(int order) {  // largest x that `order` nodes cover
     double f = 1.0;
@@ -1479,8 +1560,6 @@ int hbin_order(double x) {
     return kHBinMaxOrder + 1;
 }
 
-double hbin_branch_point(int basis) { return basis == kSph ? (double)0.06f : (double)0.24f; }
-
 // The largest |k| of a half-spectrum lattice and the largest a^2 + b^2 + c^2.
 long long lattice_nsq(const Lattice& L) {
     const long long hx = L.nx / 2, hy = L.ny / 2, hz = L.nz - 1;
@@ -1496,12 +1575,11 @@ double hbin_unit_cost(int order, int period) {
 }
 
 // Bins of a group on a lattice: runs of fine bins chosen by dynamic
-// programming to minimise sum(count x hbin_unit_cost) + job_cost per
-// non-empty bin (a bin is one more job: its items, pipeline fills and
-// accumulator dumps), each bin's Chebyshev interval the span of its non-empty
-// fine bins.
-HBinPlan hbin_plan_build(const HBinStats& hs, int basis, double kmax, int period, int job_cost) {
-    const double r0 = hbin_branch_point(basis);
+// programming to minimise, per non-empty bin, count x hbin_unit_cost (the
+// tensor work) + order x block_cost (the reduction reads every Chebyshev
+// block at every frequency) + job_cost (items, pipeline fills), each bin's
+// Chebyshev interval the span of its non-empty fine bins.
+HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_cost, int block_cost) {
     const int F = kHBinFine;
     std::vector<long long> cum(F + 1, 0);
     for (int f = 0; f < F; ++f) cum[f + 1] = cum[f] + hs.count[f];
@@ -1518,11 +1596,10 @@ HBinPlan hbin_plan_build(const HBinStats& hs, int basis, double kmax, int period
             if (n > 0) {
                 const double lo = hs.edges[first_ne[i]], hi = hs.edges[last_ne[j] + 1];
                 order = hbin_order(kmax * (hi - lo));
-                // wider runs (smaller i) only need more nodes and are wider still
-                if (order > kHBinMaxOrder) break;
-                if (kmax * hi > r0 && hi > lo * (1.0 + kHBinKinkWidth)) break;
+                if (order > kHBinMaxOrder) break;  // wider runs (smaller i) only need more
             }
-            const double c = best[i] + (double)n * hbin_unit_cost(order, period) + (n > 0 ? job_cost : 0);
+            const double c =
+                best[i] + (n > 0 ? (double)n * hbin_unit_cost(order, period) + (double)order * block_cost + job_cost : 0.0);
             if (c < best[j]) {
                 best[j] = c;
                 arg[j] = i;
@@ -1565,25 +1642,29 @@ HBinPlan hbin_plan_build(const HBinStats& hs, int basis, double kmax, int period
 
 // Plans are cached per registration, lattice and job cost.
 std::mutex g_hbin_mu;
-std::map<std::tuple<unsigned long long, long long, double, int>, std::shared_ptr<const HBinPlan>> g_hbin_cache;
+std::map<std::tuple<unsigned long long, long long, double, long long>, std::shared_ptr<const HBinPlan>> g_hbin_cache;
 
 std::shared_ptr<const HBinPlan> hbin_plan(const SumRequest& r) {
     const long long nsq = lattice_nsq(r.lat);
     const double kmax = r.lat.kx * std::sqrt((double)nsq);
-    // MV_HBIN_JOB_COST (0 .. 1e6) replaces the tuned price of one more bin
-    static const int env_cost = [] {
-        const char* e = std::getenv("MV_HBIN_JOB_COST");
+    // MV_HBIN_JOB_COST and MV_HBIN_BLOCK_COST (0 .. 1e6) replace the tuned
+    // price of one more bin and of one more Chebyshev block
+    auto env = [](const char* name) {
+        const char* e = std::getenv(name);
         const long v = e ? std::atol(e) : -1;
         return (v >= 0 && v <= 1000000) ? (int)v : -1;
-    }();
-    const int job_cost = env_cost >= 0 ? env_cost : std::max(0, active_tune().hbin_job_cost);
+    };
+    static const int env_job = env("MV_HBIN_JOB_COST"), env_block = env("MV_HBIN_BLOCK_COST");
+    const int job_cost = env_job >= 0 ? env_job : std::max(0, active_tune().hbin_job_cost);
+    const int block_cost = env_block >= 0 ? env_block : std::max(0, active_tune().hbin_block_cost);
     const int period = r.lat.nz - 1;
-    const auto key = std::make_tuple(r.hbins->id, (nsq * 65536 + period) * 4 + r.basis, r.lat.kx, job_cost);
+    const auto key = std::make_tuple(r.hbins->id, (nsq * 65536 + period) * 4 + r.basis, r.lat.kx,
+                                     (long long)job_cost * 2000003LL + block_cost);
     std::lock_guard<std::mutex> lock(g_hbin_mu);
     auto it = g_hbin_cache.find(key);
     if (it != g_hbin_cache.end()) return it->second;
     if (g_hbin_cache.size() >= 256) g_hbin_cache.clear();
-    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, r.basis, kmax, period, job_cost));
+    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, period, job_cost, block_cost));
     g_hbin_cache[key] = plan;
     return plan;
 }
@@ -1679,9 +1760,16 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         const long long target = (long long)(device_sm_count() / ctas) * active_tune().tc_waves;
         long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
         splits = std::min<long long>(splits, std::max<long long>(1, (j.n + 64 * kKp - 1) / (64 * kKp)));
+        // an item keeps its whole sum in an FP32 total: at most kMaxItemChains chains
+        const int flush_stages = narrow_mode(mode) ? plan.flush_narrow : plan.flush;
+        const long long max_chunk = (long long)kMaxItemChains * flush_stages * kKp;
+        splits = std::max<long long>(splits, (j.n + max_chunk - 1) / max_chunk);
         const long long chunk = ((j.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
         splits = (j.n + chunk - 1) / chunk;
         j.k_chunk = (int)chunk;
+        j.n_splits = (int)splits;
+        j.ctas = ctas;
+        j.slot_stride = ctas * kM * 2 * j.nc_tile;
         j.n_blocks = (j.n + kBlockParticles - 1) / kBlockParticles;
         j.img_stride = 512 * (j.nc_tile / ctas);
         j.bimg = nullptr;
@@ -1698,6 +1786,20 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         plan.job_class.push_back(cls);
         plan.job_acc.push_back(acc_part);
         plan.job_coef.push_back(coef_offset);
+        plan.job_slot.push_back(plan.slot_floats);
+        plan.slot_floats += (size_t)(splits * ftiles) * (size_t)j.slot_stride;
+        // column c of the job -> its n-tile and the slot columns of its Re and
+        // Im parts (the accumulator's column order: per CTA half h of the
+        // n-tile's c values, Re of its bnc values, then Im)
+        plan.job_colmap.push_back(plan.colmaps.size());
+        for (int c = 0; c < j.lz_tc; ++c) {
+            const int n_tile = c / j.nc_tile, c_in = c - n_tile * j.nc_tile;
+            const int bnc = std::min(j.nc_tile, j.lz_tc - n_tile * j.nc_tile) / ctas;
+            const int h = c_in / bnc, cc = c_in - h * bnc;
+            plan.colmaps.push_back(make_int4(n_tile, h * 2 * bnc + cc, h * 2 * bnc + bnc + cc, 0));
+        }
+        TensorPlan::Class& cl = plan.classes[cls];
+        (acc_part == 0 ? cl.jobs : acc_part == 1 ? cl.nyq_pos : cl.nyq_neg).push_back(job_index);
         const int flush = narrow_mode(mode) ? plan.flush_narrow : plan.flush;
         for (long long ks = 0; ks < splits; ++ks) {
             const long long k0 = ks * chunk, k1 = std::min<long long>(j.n, k0 + chunk);
@@ -1740,10 +1842,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             c.h = key.h;
             c.factored = !key.unfactored;
             c.scale = r.scale;
-            c.acc_offset = plan.acc_bytes;
-            plan.acc_bytes += ((size_t)kx * ky * lz_tc * 2 * sizeof(double) + 255) / 256 * 256;
             c.nyquist = false;
-            c.acc_nyq_offset = 0;
             plan.classes.push_back(c);
         }
         plan.group_class.push_back(cls);
@@ -1756,15 +1855,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             continue;
         }
         const bool nyq_ok = ky % 16 == 0 && kx % 2 == 0 && (kx / 2) % 8 == 0;
-        // the Nyquist plane's accumulator, once per class
-        auto class_nyquist = [&]() {
-            TensorPlan::Class& c = plan.classes[cls];
-            if (!c.nyquist) {
-                c.nyquist = true;
-                c.acc_nyq_offset = plan.acc_bytes;
-                plan.acc_bytes += ((size_t)kx * ky * 2 * sizeof(double) + 255) / 256 * 256;
-            }
-        };
+        // the class's Nyquist plane comes from transposed jobs
+        auto class_nyquist = [&]() { plan.classes[cls].nyquist = true; };
         if (binned) {
             // ------------------------------------------ h-binned group
             const std::shared_ptr<const HBinPlan> hp = hbin_plan(r);
@@ -1778,17 +1870,19 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             bg.meta_offset = 0;  // placed by tensor_reserve_upload
             bg.cursor_offset = plan.acc_bytes;
             plan.acc_bytes += ((size_t)bg.nbins * sizeof(int) + 255) / 256 * 256;
+            bg.sorted_offset = plan.sorted_bytes;
+            plan.sorted_bytes += ((size_t)r.n * sizeof(float4) + 255) / 256 * 256 + ((size_t)r.n * sizeof(float) + 255) / 256 * 256;
             bg.coef_offset = plan.coef_bytes / sizeof(float);
-            size_t coef_count = 0;
             std::vector<int> first_block(bg.nbins);
             long long blocks = 0;
+            bg.total_q = 0;
             for (int b = 0; b < bg.nbins; ++b) {
                 first_block[b] = (int)blocks;
                 blocks += (bg.bins[b].count + kBlockParticles - 1) / kBlockParticles;
-                coef_count += (size_t)bg.bins[b].order * bg.nsq;
+                bg.total_q += bg.bins[b].order;
             }
-            bg.coef_count = coef_count;
-            plan.coef_bytes += (coef_count * sizeof(float) + 255) / 256 * 256;
+            bg.coef_count = (size_t)bg.total_q * bg.nsq;  // [n2][bin's blocks]
+            plan.coef_bytes += (bg.coef_count * sizeof(float) + 255) / 256 * 256;
             const size_t blocks_bytes = (size_t)blocks * kBlockBytes;
             plan.tp_bytes += blocks_bytes;
             // the Nyquist plane as transposed jobs needs whole 8-c blocks of
@@ -1803,8 +1897,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             int first_job = -1, first_nyq = -1;
             for (int b = 0; b < bg.nbins; ++b) {
                 const HBin& bin = bg.bins[b];
-                const size_t coef_off = bg.coef_offset + coef_at;
-                coef_at += (size_t)bin.order * bg.nsq;
+                const size_t coef_off = bg.coef_offset + coef_at;  // the bin's first block, within one |k|^2
+                coef_at += (size_t)bin.order;
                 if (bin.count <= 0 || !(bin.wmax > 0.f)) continue;
                 TcJob j{};
                 j.kx = kx;
@@ -1817,7 +1911,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
                 j.gauss = 0;
                 j.wmax = bin.wmax;
                 j.period = lz_tc;
-                j.coef_stride = bg.nsq;
+                j.coef_stride = bg.total_q;
                 const size_t tp = plan.tp_offset.back() + (size_t)first_block[b] * kBlockBytes;
                 const int jm = add_job(j, mode_of(j.lz_tc, (long long)kx * ky), true, tp, cls, 0, coef_off);
                 if (first_job < 0) first_job = jm;
@@ -1917,11 +2011,33 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     }
     const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
     plan.meta_bytes = jobs_bytes + ((plan.items.size() * sizeof(int2) + 255) / 256) * 256;
-    // the binned groups' tables: edges, int4 bins, float4 spans (16-byte aligned)
+    // the jobs with B-operand images and their first images
+    plan.img_jobs.clear();
+    plan.img_first.assign(1, 0);
+    for (size_t j = 0; j < plan.jobs.size(); ++j) {
+        if (plan.bimg_offset[j] == SIZE_MAX) continue;
+        const TcJob& J = plan.jobs[j];
+        plan.img_jobs.push_back((int)j);
+        plan.img_first.push_back(plan.img_first.back() + (long long)J.n_ntiles * J.ctas * J.n_blocks);
+    }
+    plan.img_jobs_offset = plan.meta_bytes;
+    plan.meta_bytes += (plan.img_jobs.size() * sizeof(int) + 255) / 256 * 256;
+    plan.img_first_offset = plan.meta_bytes;
+    plan.meta_bytes += (plan.img_first.size() * sizeof(long long) + 255) / 256 * 256;
+    // the jobs' column maps
+    plan.colmap_offset = plan.meta_bytes;
+    plan.meta_bytes += (plan.colmaps.size() * sizeof(int4) + 255) / 256 * 256;
+    // each class's job lists (planes, Nyquist a >= 0, Nyquist a < 0)
+    for (TensorPlan::Class& c : plan.classes) {
+        c.list_offset = plan.meta_bytes;
+        plan.meta_bytes += ((c.jobs.size() + c.nyq_pos.size() + c.nyq_neg.size()) * sizeof(int) + 255) / 256 * 256;
+    }
+    // the binned groups' tables: edges, int4 bins, float4 spans, int first
+    // particles (16-byte aligned)
     for (TensorPlan::Binned& bg : plan.binned) {
         bg.meta_offset = plan.meta_bytes;
         const size_t edges = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
-        plan.meta_bytes += edges + (size_t)bg.nbins * (sizeof(int4) + sizeof(float4));
+        plan.meta_bytes += edges + (size_t)bg.nbins * (sizeof(int4) + sizeof(float4)) + (size_t)(bg.nbins + 1) * sizeof(int);
         plan.meta_bytes = (plan.meta_bytes + 255) / 256 * 256;
     }
     return kOk;
@@ -1933,43 +2049,56 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     if (st == kOk) st = ws.meta.reserve(std::max<size_t>(plan.meta_bytes, 256));
     if (st == kOk && plan.bimg_bytes) st = ws.bimg.reserve(plan.bimg_bytes);
     if (st == kOk && plan.coef_bytes) st = ws.coef.reserve(plan.coef_bytes);
+    if (st == kOk && plan.sorted_bytes) st = ws.sorted.reserve(plan.sorted_bytes);
+    if (st == kOk) st = ws.slots.reserve(std::max<size_t>(plan.slot_floats * sizeof(float), 256));
     if (st != kOk) return st;
     char* tp_base = static_cast<char*>(ws.particles.ptr);
-    char* acc_base = static_cast<char*>(ws.acc.ptr);
     for (size_t j = 0; j < plan.jobs.size(); ++j) {
         TcJob& job = plan.jobs[j];
         job.bimg = plan.bimg_offset[j] == SIZE_MAX ? nullptr
                                                    : static_cast<const unsigned char*>(ws.bimg.ptr) + plan.bimg_offset[j];
         job.blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.job_tp[j]);
-        const TensorPlan::Class& c = plan.classes[plan.job_class[j]];
-        // Nyquist jobs: the a < 0 job's Kx/2 columns come first in the
-        // accumulator, then the a >= 0 job's
-        double* nyq_acc = reinterpret_cast<double*>(acc_base + c.acc_nyq_offset);
-        job.acc = plan.job_acc[j] == 0   ? reinterpret_cast<double*>(acc_base + c.acc_offset)
-                  : plan.job_acc[j] == 1 ? nyq_acc + (size_t)(c.kx / 2) * 2 * c.ky
-                                         : nyq_acc;
+        job.slots = static_cast<float*>(ws.slots.ptr) + plan.job_slot[j];
+        job.colmap = reinterpret_cast<const int4*>(static_cast<char*>(ws.meta.ptr) + plan.colmap_offset) +
+                     plan.job_colmap[j];
         job.coef = plan.job_coef[j] == SIZE_MAX ? nullptr : static_cast<const float*>(ws.coef.ptr) + plan.job_coef[j];
     }
     std::vector<char> meta(plan.meta_bytes, 0);
     const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
     if (!plan.jobs.empty()) std::memcpy(meta.data(), plan.jobs.data(), plan.jobs.size() * sizeof(TcJob));
     if (!plan.items.empty()) std::memcpy(meta.data() + jobs_bytes, plan.items.data(), plan.items.size() * sizeof(int2));
+    if (!plan.colmaps.empty())
+        std::memcpy(meta.data() + plan.colmap_offset, plan.colmaps.data(), plan.colmaps.size() * sizeof(int4));
+    if (!plan.img_jobs.empty()) {
+        std::memcpy(meta.data() + plan.img_jobs_offset, plan.img_jobs.data(), plan.img_jobs.size() * sizeof(int));
+        std::memcpy(meta.data() + plan.img_first_offset, plan.img_first.data(), plan.img_first.size() * sizeof(long long));
+    }
+    for (const TensorPlan::Class& c : plan.classes) {
+        int* l = reinterpret_cast<int*>(meta.data() + c.list_offset);
+        for (int v : c.jobs) *l++ = v;
+        for (int v : c.nyq_pos) *l++ = v;
+        for (int v : c.nyq_neg) *l++ = v;
+    }
     for (const TensorPlan::Binned& bg : plan.binned) {
         float* edges = reinterpret_cast<float*>(meta.data() + bg.meta_offset);
         const size_t edges_bytes = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
         int4* bins = reinterpret_cast<int4*>(meta.data() + bg.meta_offset + edges_bytes);
         float4* spans = reinterpret_cast<float4*>(bins + bg.nbins);
-        int block = 0;
-        size_t coef_at = bg.coef_offset;
+        int* first = reinterpret_cast<int*>(spans + bg.nbins);
+        int block = 0, particle = 0;
+        int coef_at = 0;
         for (int b = 0; b < bg.nbins; ++b) {
             const HBin& bin = bg.bins[b];
             edges[b] = bg.edges[b];
-            bins[b] = make_int4(block, bin.count, (int)coef_at, bin.order);
+            bins[b] = make_int4(block, bin.count, coef_at, bin.order);
             spans[b] = make_float4(bin.lo, bin.hi, bin.wmax > 0.f ? kOperandScale / bin.wmax : 0.f, 0.f);
+            first[b] = particle;
             block += (bin.count + kBlockParticles - 1) / kBlockParticles;
-            coef_at += (size_t)bin.order * bg.nsq;
+            particle += bin.count;
+            coef_at += bin.order;
         }
         edges[bg.nbins] = bg.edges[bg.nbins];
+        first[bg.nbins] = particle;
     }
     plan.d_jobs = static_cast<const void*>(ws.meta.ptr);
     plan.d_items = static_cast<const void*>(static_cast<char*>(ws.meta.ptr) + jobs_bytes);
@@ -2027,6 +2156,17 @@ int launch_tile(const TcArgs& a, cudaStream_t stream) {
 
 }  // namespace
 
+namespace {
+// Dynamic shared memory of the reduction kernels: the class's job
+// descriptors (and the planes kernel's partial sums).
+int reduce_smem(void (*kernel)(TcReduceArgs), size_t bytes) {
+    if (bytes > 200 * 1024) return set_error(kInvalidValue, "tensor sum: too many jobs in one output class");
+    if (bytes <= 48 * 1024) return kOk;
+    return check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                      "cudaFuncSetAttribute(reduction)");
+}
+}  // namespace
+
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag) {
     int st = kOk;
@@ -2066,6 +2206,10 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             bp.cursors = reinterpret_cast<int*>(static_cast<char*>(ws.acc.ptr) + bg.cursor_offset);
             bp.out = reinterpret_cast<uint8_t*>(tp);
             bp.out_nyq = reinterpret_cast<uint8_t*>(tpn);
+            bp.first = reinterpret_cast<const int*>(bp.spans + bg.nbins);
+            char* sorted = static_cast<char*>(ws.sorted.ptr) + bg.sorted_offset;
+            bp.sorted = reinterpret_cast<float4*>(sorted);
+            bp.sorted_radii = reinterpret_cast<float*>(sorted + ((size_t)r.n * sizeof(float4) + 255) / 256 * 256);
             bp.error_flag = error_flag;
             tc_prep_binned_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(bp);
             count_launch();
@@ -2074,9 +2218,12 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             ca.step = r.lat.kx;
             ca.nbins = bg.nbins;
             ca.nsq = bg.nsq;
+            ca.total_q = bg.total_q;
             ca.bins = bp.bins;
             ca.spans = bp.spans;
-            ca.coef = static_cast<float*>(ws.coef.ptr);
+            ca.edges = bp.edges;
+            ca.r0 = (float)phi_branch_point(r.basis);
+            ca.coef = static_cast<float*>(ws.coef.ptr) + bg.coef_offset;
             const long long entries = (long long)bg.nbins * bg.nsq;
             tc_coef_kernel<<<(unsigned)((entries + 127) / 128), 128, 0, stream>>>(ca);
             count_launch();
@@ -2099,26 +2246,21 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
     }
     st = check_cuda(cudaGetLastError(), "tc_prep_kernel launch");
     if (st != kOk) return st;
-    // B-operand images (after the constants they are made from)
-    for (const TcJob& j : plan.jobs) {
-        if (!j.bimg) continue;
+    // B-operand images of every job that has them, in one launch (after the
+    // constants they are made from)
+    if (!plan.img_jobs.empty()) {
         TcImageArgs ia;
-        ia.blocks = j.blocks;
-        ia.bimg = const_cast<unsigned char*>(j.bimg);
-        ia.n_blocks = j.n_blocks;
-        ia.img_stride = j.img_stride;
-        ia.ctas = j.img_stride == 512 * j.nc_tile ? 1 : 2;  // 512 nc_tile bytes for one CTA, half for a pair
-        ia.nc_tile = j.nc_tile;
-        ia.lz_tc = j.lz_tc;
-        ia.c_base = j.c_base;
-        ia.period = j.period;
-        ia.gauss = j.gauss != 0;
-        const long long images = (long long)j.n_ntiles * ia.ctas * j.n_blocks;
+        ia.jobs = static_cast<const TcJob*>(plan.d_jobs);
+        ia.img_jobs = reinterpret_cast<const int*>(static_cast<const char*>(ws.meta.ptr) + plan.img_jobs_offset);
+        ia.img_first = reinterpret_cast<const long long*>(static_cast<const char*>(ws.meta.ptr) + plan.img_first_offset);
+        ia.n_img_jobs = (int)plan.img_jobs.size();
+        const long long images = plan.img_first.back();
+        if (images > 0x7fffffffLL) return set_error(kInvalidValue, "tensor sum: too many B-operand images");
         tc_bimg_kernel<<<(unsigned)images, 256, 0, stream>>>(ia);
         count_launch();
+        st = check_cuda(cudaGetLastError(), "tc_bimg_kernel launch");
+        if (st != kOk) return st;
     }
-    st = check_cuda(cudaGetLastError(), "tc_bimg_kernel launch");
-    if (st != kOk) return st;
     // one persistent launch per tile mode for all groups
     if (!plan.items.empty()) {
         timer_begin(timer, 3, stream);
@@ -2158,10 +2300,15 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         timer_end(timer, 3, stream);
         if (st != kOk) return st;
     }
-    // FP64 accumulators -> spectra (added to what is there)
+    // the items' tiles -> spectra, summed in FP64 (added to what is there)
     for (const TensorPlan::Class& c : plan.classes) {
-        TcFinalizeArgs f;
-        f.acc = reinterpret_cast<const double*>(static_cast<const char*>(ws.acc.ptr) + c.acc_offset);
+        const int* lists = reinterpret_cast<const int*>(static_cast<const char*>(ws.meta.ptr) + c.list_offset);
+        TcReduceArgs f;
+        f.jobs = static_cast<const TcJob*>(plan.d_jobs);
+        f.list = lists;
+        f.n_list = (int)c.jobs.size();
+        f.list_neg = nullptr;
+        f.n_neg = 0;
         f.kx = c.kx;
         f.ky = c.ky;
         f.lz_tc = c.lz_tc;
@@ -2172,21 +2319,54 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         f.factored = c.factored;
         f.scale = c.scale;
         f.out = c.out;
-        f.accumulate = true;
         f.nyquist = false;
-        const long long count = (long long)c.kx * c.ky * c.lz_tc;
-        tc_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(f);
-        count_launch();
+        if (f.n_list > 0) {
+            const long long blocks = ((long long)c.kx * c.ky + 31) / 32 * (c.lz_tc / kReduceC);
+            const size_t smem = (((size_t)f.n_list * sizeof(ReduceJob) + 15) & ~(size_t)15) +
+                                (size_t)kReduceWarps * 32 * kReduceC * sizeof(double2);
+            st = reduce_smem(tc_reduce_planes_kernel, smem);
+            if (st != kOk) return st;
+            tc_reduce_planes_kernel<<<(unsigned)blocks, 32 * kReduceWarps, smem, stream>>>(f);
+            count_launch();
+        }
         if (c.nyquist) {
-            f.acc = reinterpret_cast<const double*>(static_cast<const char*>(ws.acc.ptr) + c.acc_nyq_offset);
+            f.list = lists + c.jobs.size();
+            f.n_list = (int)c.nyq_pos.size();
+            f.list_neg = lists + c.jobs.size() + c.nyq_pos.size();
+            f.n_neg = (int)c.nyq_neg.size();
             f.nyquist = true;
             const long long plane = (long long)c.kx * c.ky;
-            tc_finalize_kernel<<<(unsigned)((plane + 255) / 256), 256, 0, stream>>>(f);
+            const size_t smem = (size_t)(f.n_list + f.n_neg) * sizeof(ReduceJob);
+            st = reduce_smem(tc_reduce_kernel, smem);
+            if (st != kOk) return st;
+            tc_reduce_kernel<<<(unsigned)((plane + 255) / 256), 256, smem, stream>>>(f);
             count_launch();
         }
     }
-    st = check_cuda(cudaGetLastError(), "tc_finalize_kernel launch");
+    st = check_cuda(cudaGetLastError(), "tc_reduce_kernel launch");
     if (st != kOk) return st;
+    // the branch part of h-binned groups with the plain form, over their
+    // particles sorted by bin
+    for (size_t g = 0; g < groups.size(); ++g) {
+        if (plan.group_binned[g] < 0 || plan.job_of_group[g] < 0) continue;
+        const TensorPlan::Binned& bg = plan.binned[plan.group_binned[g]];
+        const char* meta = static_cast<const char*>(ws.meta.ptr) + bg.meta_offset;
+        const size_t edges_bytes = ((size_t)(bg.nbins + 1) * sizeof(float) + 15) / 16 * 16;
+        const char* sorted = static_cast<const char*>(ws.sorted.ptr) + bg.sorted_offset;
+        SumRequest k = groups[g];
+        k.particles = reinterpret_cast<const float4*>(sorted);
+        k.radii = reinterpret_cast<const float*>(sorted + ((size_t)k.n * sizeof(float4) + 255) / 256 * 256);
+        k.accumulate = true;
+        k.kink = 1;
+        k.shell_edges = reinterpret_cast<const float*>(meta);
+        k.shell_first = reinterpret_cast<const int*>(meta + edges_bytes + (size_t)bg.nbins * (sizeof(int4) + sizeof(float4)));
+        k.shell_nbins = bg.nbins;
+        // without transposed Nyquist jobs the plain form sums the whole Nyquist
+        // plane below (branch included): leave it out here
+        if (plan.nyq_job_of_group[g] < 0) k.lat.nz -= 1;
+        st = launch_plain_sum(k, plain_ws, timer);
+        if (st != kOk) return st;
+    }
     // the Nyquist plane l = Kz/2 with the plain form, for groups without a
     // transposed job (groups without particles or weight have neither)
     for (size_t g = 0; g < groups.size(); ++g) {
