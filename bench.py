@@ -68,9 +68,10 @@ def sum_terms_split(w):
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from ncu
-# captures of dram__bytes_read.sum + dram__bytes_write.sum (profiles/*.md
-# names the capture and its command); None where no capture exists.
-DRAM_TRAFFIC_PER_LAUNCH = {}
+# captures of dram__bytes_read.sum + dram__bytes_write.sum of the full-size
+# launch (profiles/tc_sum_kernel_c3_dram.md names the capture and its
+# command); None where no capture exists.
+DRAM_TRAFFIC_PER_LAUNCH = {("C3", "tc_sum_kernel"): 21.89e9 + 4.44e9}
 
 
 def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
@@ -81,7 +82,6 @@ def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
     terms, n, g = terms_per_step(w)
     (p_ms, p_n), (t_ms, t_n) = stage_t[0], stage_t[3]
     max_mhz = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
-    traffic = DRAM_TRAFFIC_PER_LAUNCH.get(w["name"])
     if t_ms > p_ms and t_n > 0:
         tc_terms, _ = sum_terms_split(w)
         per_launch_terms = tc_terms * steps / t_n
@@ -91,7 +91,8 @@ def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
         peak = peaks.get("bf16_tflops_sustained", 1400.0)
         burst = peaks.get("bf16_tflops", 1590.0)
         return {"bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak,
-                "traffic": traffic, "kernel": "tc_sum_kernel", "flops_per_term": 8,
+                "traffic": DRAM_TRAFFIC_PER_LAUNCH.get((w["name"], "tc_sum_kernel")), "kernel": "tc_sum_kernel",
+                "flops_per_term": 8,
                 "issued_tflops": issued, "issued_frac": issued / peak, "issued_frac_of_burst": issued / burst,
                 "issued_note": "3 FP16 products per term (hi*hi, hi*lo, lo*hi): 24 issued flops per term",
                 "terms_per_launch": per_launch_terms, "launch_ms": t_ms / t_n, "launches": t_n,
@@ -101,7 +102,8 @@ def sum_roofline(stage_t, w, steps, peaks, peak_src, clk, sm_count):
     launch_s = p_ms / max(1, p_n) / 1000.0
     alg = 8.0 * per_launch_terms / launch_s / 1e12 if launch_s > 0 else 0.0
     peak = sm_count * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
-    r = {"bound": "fp32", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak, "traffic": traffic,
+    r = {"bound": "fp32", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak,
+         "traffic": DRAM_TRAFFIC_PER_LAUNCH.get((w["name"], "fold_sum_kernel")),
          "kernel": "fold_sum_kernel", "flops_per_term": 8, "terms_per_launch": per_launch_terms,
          "launch_ms": p_ms / max(1, p_n), "launches": p_n,
          "peak_source": f"nominal FP32: {sm_count} SMs x {FP32_LANES_PER_SM} lanes x 2 flop x {max_mhz:.0f} MHz "

@@ -900,11 +900,10 @@ int vis_spectrum_compute(VisSpectrum* sp, VisConfig* c, MeshlessDataset* ds, int
     int rc = check_cuda(cudaMemsetAsync(sp->data, 0, sizeof(float2) * sp->count, s->stream), "cudaMemsetAsync");
     if (rc != kOk) return rc;
     if (!tc_groups.empty()) {
-        TensorPlan plan;
-        rc = tensor_plan(tc_groups, plan);
-        if (rc == kOk) rc = tensor_reserve_upload(plan, s->tensor, s->stream);
+        const TensorPlan* plan = nullptr;
+        rc = tensor_prepare(tc_groups, s->tensor, s->stream, &plan);
         if (rc == kOk)
-            rc = tensor_enqueue(tc_groups, plan, s->tensor, s->partials, &s->timer, s->stream,
+            rc = tensor_enqueue(tc_groups, *plan, s->tensor, s->partials, &s->timer, s->stream,
                                 static_cast<int*>(s->error_word.ptr));
         if (rc != kOk) return rc;
     }

@@ -154,8 +154,8 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 //   tensor_reserve_upload grows the workspaces and uploads the job and item
 //                         tables (not capturable in a CUDA graph);
 //   tensor_enqueue        per-particle constants, the persistent launch (each
-//                         work item stores its FP32 tile), the FP64 reduction
-//                         of the tiles into the spectra (added), the Nyquist
+//                         work item writes its totals into its slot), the FP64
+//                         reduction of the slots into the spectra (added), the Nyquist
 //                         planes of groups without a Nyquist job and the
 //                         branch part of h-binned groups (plain form, added);
 //                         stream-ordered and capturable once the workspaces
@@ -165,7 +165,7 @@ int launch_slice_extract_batch(const SliceView* d_views, int number_of_views, lo
 int tensor_sum_available(const SumRequest& req, int form);
 
 // One job of the persistent tensor-core kernel: a separable group summed over
-// a lattice of rows (a, b) and columns c >= 0 into an FP64 accumulator.  Its
+// a lattice of rows (a, b) and columns c >= 0 into its work items' slots.  Its
 // work items are (split ks, m tile, n tile), local index (ks * n_mtiles +
 // m_tile) * n_ntiles + n_tile.  Device-resident.
 //
@@ -187,13 +187,17 @@ int tensor_sum_available(const SumRequest& req, int form);
 // per stage.
 struct TcJob {
     const unsigned char* blocks;  // the job's per-particle constants, 32-particle blocks
-    // Item results: each work item stores its FP32 tile once, at its end, into
-    // slots[local item * slot_stride ..]: per CTA of the item (rank r at
-    // r * 128 * 2 nc_tile) its 128 rows of every accumulator column n, in
-    // quads of columns: [n / 4][row][n % 4].
-    // tc_reduce_kernel sums them over the items of every job in FP64.
-    float* slots;
-    int slot_stride;  // floats per item: ctas * 128 * 2 nc_tile
+    // Item results: each work item owns slot [local item * slot_stride ..] of
+    // `slots`: per CTA of the item (rank r at r * 128 * 2 nc_tile elements)
+    // its 128 rows of every accumulator column n.  A job whose items span at
+    // most 64 accumulation chains stores each item's FP32 total once, in
+    // quads of columns ([n / 4][row][n % 4] floats); a job with longer items
+    // (slot_fp64) adds the item's FP32 total of every 64 chains into FP64
+    // totals, in pairs of columns ([n / 2][row][n % 2] doubles).
+    // tc_reduce_kernel sums the slots over the items of every job in FP64.
+    void* slots;
+    int slot_stride;  // elements per item: ctas * 128 * 2 nc_tile
+    int slot_fp64;
     int n_splits;     // particle chunks (items per tile)
     int ctas;         // 2 for the CTA-pair tiles
     double wmax;
@@ -285,7 +289,7 @@ struct TensorPlan {
     // per job: its particle constants (offset into the particles workspace),
     // accumulator class and part (0 planes, 1 Nyquist a >= 0, 2 Nyquist a < 0),
     // coefficient table (offset in floats into coef, SIZE_MAX for none)
-    std::vector<size_t> job_tp, job_coef, job_slot;  // job_slot: offset in floats into slots
+    std::vector<size_t> job_tp, job_coef, job_slot;  // job_slot: byte offset into slots
     std::vector<size_t> job_colmap;                 // the job's column map: index into colmaps
     std::vector<int4> colmaps;                      // all jobs' column maps
     size_t colmap_offset = 0;                       // colmaps in meta
@@ -293,7 +297,7 @@ struct TensorPlan {
     std::vector<long long> img_first;               // their first images (and the total last)
     size_t img_jobs_offset = 0, img_first_offset = 0;  // both in meta
     std::vector<int> job_class, job_acc;
-    size_t slot_floats = 0;
+    size_t slot_bytes = 0;
     std::vector<size_t> tp_offset, tp_nyq_offset;
     std::vector<size_t> bimg_offset;  // per job: its B-operand images in the workspace, or SIZE_MAX
     size_t bimg_bytes = 0;
@@ -307,16 +311,21 @@ struct TensorPlan {
 struct TensorWorkspace {
     Workspace particles;  // per-particle constants of every group
     Workspace acc;        // per-compute counters (zeroed each compute)
-    Workspace slots;      // work items' FP32 tiles
+    Workspace slots;      // work items' totals (FP32 or FP64)
     Workspace meta;       // job and item tables
     Workspace bimg;       // B-operand images
     Workspace coef;       // Chebyshev coefficient tables of h-binned groups
     Workspace sorted;     // h-binned groups' particles and radii sorted by bin
     std::vector<char> uploaded;  // the tables last copied to `meta`
     void* uploaded_to = nullptr;
+    // the last plan made here (tensor_prepare), uploaded, and what it was made of
+    std::string plan_key;
+    std::unique_ptr<TensorPlan> plan;
     void release() {
         uploaded.clear();
         uploaded_to = nullptr;
+        plan_key.clear();
+        plan.reset();
         particles.release();
         acc.release();
         slots.release();
@@ -334,6 +343,11 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan);
 // eighth of the current device's memory.
 size_t operand_cache_limit();
 int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream);
+// tensor_plan + tensor_reserve_upload, skipped when the groups, the launch
+// parameters in force and the device are those of the workspace's last plan
+// (a compute repeated on the same registered data); *plan points into ws.
+int tensor_prepare(const std::vector<SumRequest>& groups, TensorWorkspace& ws, cudaStream_t stream,
+                   const TensorPlan** plan);
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag);
 

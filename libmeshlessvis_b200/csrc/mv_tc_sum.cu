@@ -25,10 +25,12 @@
 // stages (a chain of flush_stages x 12 MMAs; the tensor core's FP32
 // accumulation loses accuracy with chain length: 1.6e-6 rel-L2 at 4 stages,
 // 2.4e-6 at 8, 4.1e-6 at 16) the MMA pauses while the flush warps add the
-// accumulator into an FP32 total in the other 256 TMEM columns.  At the end
-// of its particle range (at most kMaxItemChains chains) a work item stores its
-// total once, with plain coalesced stores, into its own slot of global memory
-// ([column][row]: a warp's rows are contiguous).  No atomics: tc_reduce_kernel
+// accumulator into an FP32 total in the other 256 TMEM columns.  A work item
+// (one particle range of one tile) owns a slot of global memory: at its end
+// an item of at most kMaxItemChains chains stores its FP32 total there once,
+// and a longer item adds its FP32 total of every kMaxItemChains chains into
+// FP64 totals there, with coalesced loads and stores (a warp's rows are
+// contiguous).  No atomics: tc_reduce_kernel
 // then sums every element's slots over particle chunks and jobs (groups,
 // h-bins) in FP64, in a fixed order, and adds the result to the float2
 // spectrum, so results are bitwise reproducible.
@@ -123,8 +125,9 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kColTotal = 256;  // FP32 total: columns [256, 256 + accumulator columns)
 constexpr float kOperandScale = 4096.f;                     // 2^12 per operand
 constexpr double kInvProductScale = 1.0 / (4096.0 * 4096.0);  // 2^-24
-// An item sums at most this many accumulation chains in its FP32 total
-// (random-walk rounding of about 2^-24 sqrt(64) of the total).
+// An FP32 total in TMEM sums at most this many accumulation chains (random-walk
+// rounding of about 2^-24 sqrt(64) of the total) before it goes to the item's
+// slot.
 constexpr int kMaxItemChains = 64;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 // After a wait has run out, a CTA idles this long before it releases TMEM and
@@ -214,7 +217,8 @@ struct TcItem {
     int period;                  // h-binned job: frequency columns per Chebyshev block (else 0)
     const unsigned char* bimg;   // this CTA's B-operand images of the item's n-tile (one per block), or null
     int img_stride, img_bytes;   // bytes between images; bytes of one image (512 bnc)
-    float* slot;                 // this CTA's part of the item's result tile: [column / 4][128 rows][column % 4]
+    void* slot;                  // this CTA's part of the item's slot (TcJob::slots)
+    int slot_fp64;               // FP64 totals ([column / 2][128 rows][column % 2]), else FP32 quads
 };
 
 template <int MODE>
@@ -245,7 +249,9 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.bimg = r.job->bimg ? r.job->bimg + (size_t)(r.n_tile * Shape<MODE>::kCtas + rank) * r.job->n_blocks *
                                              (size_t)r.img_stride
                          : nullptr;
-    r.slot = r.job->slots + (size_t)v.y * r.job->slot_stride + (size_t)rank * kM * 2 * r.job->nc_tile;
+    r.slot_fp64 = r.job->slot_fp64;
+    r.slot = static_cast<char*>(r.job->slots) +
+             ((size_t)v.y * r.job->slot_stride + (size_t)rank * kM * 2 * r.job->nc_tile) * (r.slot_fp64 ? 8 : 4);
     return r;
 }
 
@@ -416,6 +422,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
         : "r"(taddr));
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ void tmem_st32(uint32_t taddr, const float* v) {
@@ -755,7 +770,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
         for (int it = unit; it < a.n_items && !__any_sync(0xffffffffu, *abort_flag != 0); it += n_units) {
             const TcItem I = tc_item<MODE>(a, it, rank);
             const int ncols = 2 * I.nc;
-            float* slot = I.slot + row * 4;  // columns n..n+3 (n % 4 == 0) at slot[(n / 4) * 512]: quads of rows
+            // FP32 slot: columns n..n+3 (n % 4 == 0) at [(n / 4) * 512 + row * 4];
+            // FP64 slot: columns n, n + 1 (n even) at [(n / 2) * 256 + row * 2]
+            float* slot32 = static_cast<float*>(I.slot) + row * 4;
+            double* slot64 = static_cast<double*>(I.slot) + row * 2;
             for (int kk = 0; kk < I.n_chunks; ++kk) {
                 const int k = C + kk;
                 const int b = k % kBufs, u = k / kBufs;
@@ -764,41 +782,71 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, a.wait_limit_ns, 4))) break;
                 tc_fence_after();
                 tmem_wait_st();  // the previous flush's stores of the total
-                // the item's chain partials are summed into an FP32 total in
-                // TMEM; the last chain's sum goes to the item's slot instead
-                const bool first = kk == 0;
-                const bool last = kk == I.n_chunks - 1;
-                // 32 columns per round trip.  ncols is a multiple of 16, so the
-                // last trip may carry 16 columns past ncols: they stay inside
-                // the accumulator and total regions and are never stored.
+                // the chain partials are summed into an FP32 total in TMEM, over
+                // at most kMaxItemChains chains; then (and at the item's end)
+                // the total goes to the item's slot instead: stored (FP32
+                // slots, items of at most kMaxItemChains chains) or added to
+                // the FP64 totals (the first time stored)
+                const bool restart = (kk % kMaxItemChains) == 0;
+                const bool dump = (kk % kMaxItemChains) == kMaxItemChains - 1 || kk == I.n_chunks - 1;
+                if (dump && I.slot_fp64) {
+                    const bool first_dump = kk < kMaxItemChains;
+                    // 8 columns per round trip; the slot's loads are issued
+                    // before the TMEM reads so their latency overlaps them
 #pragma unroll 1
-                for (int cc = 0; cc < ncols; cc += 32) {
-                    float tt[32];
-                    if (first) {
-                        tmem_ld32(acc_col + cc, tt);
-                        tmem_wait_ld();
-                    } else {
-                        float dv[32];
-                        tmem_ld32(acc_col + cc, dv);
-                        tmem_ld32(lane_base + kColTotal + cc, tt);
+                    for (int cc = 0; cc < ncols; cc += 8) {
+                        double2 sv[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            sv[i] = first_dump ? make_double2(0.0, 0.0)
+                                               : __ldcg(reinterpret_cast<const double2*>(slot64 + (size_t)(cc + 2 * i) * kM));
+                        float dv[8], tv[8];
+                        tmem_ld8(acc_col + cc, dv);
+                        if (!restart) tmem_ld8(lane_base + kColTotal + cc, tv);
                         tmem_wait_ld();
 #pragma unroll
-                        for (int i = 0; i < 32; i += 2) {
-                            const float2 t2 = __fadd2_rn(make_float2(tt[i], tt[i + 1]), make_float2(dv[i], dv[i + 1]));
-                            tt[i] = t2.x;
-                            tt[i + 1] = t2.y;
+                        for (int i = 0; i < 4; ++i) {
+                            const float t0 = restart ? dv[2 * i] : tv[2 * i] + dv[2 * i];
+                            const float t1 = restart ? dv[2 * i + 1] : tv[2 * i + 1] + dv[2 * i + 1];
+                            __stcg(reinterpret_cast<double2*>(slot64 + (size_t)(cc + 2 * i) * kM),
+                                   make_double2(sv[i].x + (double)t0, sv[i].y + (double)t1));
                         }
                     }
-                    if (!last) {
-                        tmem_st32(lane_base + kColTotal + cc, tt);
-                    } else {
-                        // ncols is a multiple of 16: whole float4 groups are in or out;
-                        // a warp's 32 rows write 512 contiguous bytes per group
+                } else {
+                    // 32 columns per round trip.  ncols is a multiple of 16, so
+                    // the last trip may carry 16 columns past ncols: they stay
+                    // inside the accumulator and total regions and are never
+                    // stored.
+#pragma unroll 1
+                    for (int cc = 0; cc < ncols; cc += 32) {
+                        float tt[32];
+                        if (restart) {
+                            tmem_ld32(acc_col + cc, tt);
+                            tmem_wait_ld();
+                        } else {
+                            float dv[32];
+                            tmem_ld32(acc_col + cc, dv);
+                            tmem_ld32(lane_base + kColTotal + cc, tt);
+                            tmem_wait_ld();
 #pragma unroll
-                        for (int i = 0; i < 32; i += 4)
-                            if (cc + i < ncols)
-                                *reinterpret_cast<float4*>(slot + (size_t)(cc + i) * kM) =
-                                    make_float4(tt[i], tt[i + 1], tt[i + 2], tt[i + 3]);
+                            for (int i = 0; i < 32; i += 2) {
+                                const float2 t2 =
+                                    __fadd2_rn(make_float2(tt[i], tt[i + 1]), make_float2(dv[i], dv[i + 1]));
+                                tt[i] = t2.x;
+                                tt[i + 1] = t2.y;
+                            }
+                        }
+                        if (!dump) {
+                            tmem_st32(lane_base + kColTotal + cc, tt);
+                        } else {
+                            // ncols is a multiple of 16: whole float4 groups are in or
+                            // out; a warp's 32 rows write 512 contiguous bytes per group
+#pragma unroll
+                            for (int i = 0; i < 32; i += 4)
+                                if (cc + i < ncols)
+                                    *reinterpret_cast<float4*>(slot32 + (size_t)(cc + i) * kM) =
+                                        make_float4(tt[i], tt[i + 1], tt[i + 2], tt[i + 3]);
+                        }
                     }
                 }
                 tc_fence_before();
@@ -1266,7 +1314,8 @@ __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
 // What the reduction needs of a job, gathered into shared memory once per
 // block (the job table's other fields are not read).
 struct ReduceJob {
-    const float* slots;
+    const void* slots;
+    int slot_fp64;
     const int4* colmap;
     const float* coef;  // null unless h-binned
     double scale;       // W x 2^-24
@@ -1279,6 +1328,7 @@ struct ReduceJob {
 __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     ReduceJob r;
     r.slots = J.slots;
+    r.slot_fp64 = J.slot_fp64;
     r.colmap = J.colmap;
     r.coef = J.period > 0 ? J.coef : nullptr;
     r.scale = J.wmax * kInvProductScale;
@@ -1297,22 +1347,41 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
 // Adds one job's contribution at lattice row rho (within the job's rows) and
 // the kC consecutive frequency columns c0 .. c0 + kC - 1 (c_idx, before the
 // Chebyshev blocks of an h-binned job; they share one n-tile and one CTA half,
-// as n-tiles and halves hold multiples of 8 columns): the FP32 tiles of all
-// its particle chunks summed in FP64, each h-binned block weighted by its
-// coefficient at |k|^2 = n2[i] step^2, times W 2^-24.
+// as n-tiles and halves hold multiples of 8 columns): the totals of all its
+// particle chunks (FP32 or FP64 slots) summed in FP64, each h-binned block
+// weighted by its coefficient at |k|^2 = n2[i] step^2, times W 2^-24.
 constexpr int kReduceC = 4;
 __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, const int* n2, int nc, double* sr,
                                            double* si, double sign_im) {
     const int m_tile = rho >> J.mrows_log2, within = rho - (m_tile << J.mrows_log2);
     const int rank = within >> 7, rl = within & (kM - 1);
-    // slot layout [column / 4][128 rows][column % 4]: column n of row rl at
-    // (n / 4) * 512 + rl * 4 + n % 4
-    const float* row = J.slots + (size_t)rank * J.rank_stride + rl * 4;
+    // FP32 slot layout [column / 4][128 rows][column % 4]: column n of row rl
+    // at (n / 4) * 512 + rl * 4 + n % 4; FP64: [column / 2][128 rows][column %
+    // 2], column n at (n / 2) * 256 + rl * 2 + n % 2
+    const size_t rbase = (size_t)rank * J.rank_stride;
+    const float* row = static_cast<const float*>(J.slots) + rbase + rl * 4;
+    const double* row64 = static_cast<const double*>(J.slots) + rbase + rl * 2;
     for (int q = 0; q < J.blocks; ++q) {
         const int4 m = __ldg(J.colmap + q * J.period + c0);  // the same for a warp's rows
         double tr[kReduceC] = {}, ti[kReduceC] = {};
         for (int ks = 0; ks < J.n_splits; ++ks) {
             const size_t li = ((size_t)ks * J.n_mtiles + m_tile) * J.n_ntiles + m.x;
+            if (J.slot_fp64) {
+                const double* v = row64 + li * J.slot_stride;
+                if (nc == kReduceC) {
+                    // two columns per load (m.y, m.z are multiples of 4)
+                    const double2 r0 = __ldg(reinterpret_cast<const double2*>(v + (size_t)m.y * kM));
+                    const double2 r1 = __ldg(reinterpret_cast<const double2*>(v + (size_t)(m.y + 2) * kM));
+                    const double2 i0 = __ldg(reinterpret_cast<const double2*>(v + (size_t)m.z * kM));
+                    const double2 i1 = __ldg(reinterpret_cast<const double2*>(v + (size_t)(m.z + 2) * kM));
+                    tr[0] += r0.x; tr[1] += r0.y; tr[2] += r1.x; tr[3] += r1.y;
+                    ti[0] += i0.x; ti[1] += i0.y; ti[2] += i1.x; ti[3] += i1.y;
+                } else {
+                    tr[0] += __ldg(v + (size_t)(m.y & ~1) * kM + (m.y & 1));
+                    ti[0] += __ldg(v + (size_t)(m.z & ~1) * kM + (m.z & 1));
+                }
+                continue;
+            }
             const float* v = row + li * J.slot_stride;
             if (nc == kReduceC) {
                 // four columns in one load (m.y, m.z are multiples of 4); a warp's
@@ -1704,10 +1773,10 @@ int tensor_sum_available(const SumRequest& r, int form) {
 
 namespace {
 
-// Groups that can share an FP64 accumulator: same output spectrum and the
-// same per-frequency factor (none for Gaussian and h-binned jobs, whose
-// factors are applied per particle or per dump; Phi^(|k| h) with the same
-// basis and h for factored ones).
+// Groups whose slots one reduction sums into one output (an output class):
+// same output spectrum and the same per-frequency factor (none for Gaussian
+// and h-binned jobs, whose factors are applied per particle or per Chebyshev
+// block; Phi^(|k| h) with the same basis and h for factored ones).
 struct ClassKey {
     const float2* out;
     int unfactored;
@@ -1754,18 +1823,26 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         // the last m-tile may extend past the rows (Nyquist jobs): the flush
         // skips rows >= kx * ky
         j.n_mtiles = (int)(((long long)j.kx * j.ky + kM * ctas - 1) / (kM * ctas));
-        // particle splits: enough items per job for ~tc_waves waves on its
-        // own (default 4), at least 64 stages each
+        // particle splits: enough items for ~tc_waves waves (default 4) of the
+        // launch, this job taking its share (the launch's groups share the
+        // waves), at least 64 stages each; every split is one more slot to
+        // write and reduce
         const long long ftiles = (long long)j.n_mtiles * j.n_ntiles;
-        const long long target = (long long)(device_sm_count() / ctas) * active_tune().tc_waves;
+        const long long target =
+            ((long long)(device_sm_count() / ctas) * active_tune().tc_waves + (long long)groups.size() - 1) /
+            std::max<long long>(1, (long long)groups.size());
         long long splits = std::max<long long>(1, (target + ftiles - 1) / ftiles);
         splits = std::min<long long>(splits, std::max<long long>(1, (j.n + 64 * kKp - 1) / (64 * kKp)));
-        // an item keeps its whole sum in an FP32 total: at most kMaxItemChains chains
+        // The 128-column tiles keep an item's whole sum in an FP32 total: at
+        // most kMaxItemChains chains per item.  The 256-column tiles take items
+        // of any length: their items add the FP32 total of every
+        // kMaxItemChains chains into FP64 totals in the slot.
         const int flush_stages = narrow_mode(mode) ? plan.flush_narrow : plan.flush;
         const long long max_chunk = (long long)kMaxItemChains * flush_stages * kKp;
-        splits = std::max<long long>(splits, (j.n + max_chunk - 1) / max_chunk);
+        if (narrow_mode(mode)) splits = std::max<long long>(splits, (j.n + max_chunk - 1) / max_chunk);
         const long long chunk = ((j.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
         splits = (j.n + chunk - 1) / chunk;
+        j.slot_fp64 = chunk > max_chunk ? 1 : 0;
         j.k_chunk = (int)chunk;
         j.n_splits = (int)splits;
         j.ctas = ctas;
@@ -1786,8 +1863,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         plan.job_class.push_back(cls);
         plan.job_acc.push_back(acc_part);
         plan.job_coef.push_back(coef_offset);
-        plan.job_slot.push_back(plan.slot_floats);
-        plan.slot_floats += (size_t)(splits * ftiles) * (size_t)j.slot_stride;
+        plan.job_slot.push_back(plan.slot_bytes);
+        plan.slot_bytes += (size_t)(splits * ftiles) * (size_t)j.slot_stride * (j.slot_fp64 ? 8 : 4);
         // column c of the job -> its n-tile and the slot columns of its Re and
         // Im parts (the accumulator's column order: per CTA half h of the
         // n-tile's c values, Re of its bnc values, then Im)
@@ -1984,9 +2061,9 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     // Per tile mode, longest first (round-robin over the persistent CTAs /
     // pairs), in cost classes 5% wide.  Within a class, items run in blocks of
     // as many m-tiles as there are resident units: one wave takes one (job,
-    // split) over distinct m-tiles, and the next waves the other jobs' items of
-    // the same m-tiles, so jobs that share an FP64 accumulator (the h-bins of a
-    // spectrum) dump into lines still held in L2 instead of re-reading them.
+    // split) over distinct m-tiles, all of them reading the same B-operand
+    // stages (images) at about the same time, and the next waves the other
+    // jobs' items of the same m-tiles.
     auto order = [](int m) { return m == kNarrow ? 0 : m == kPairNarrow ? 1 : m == kPair ? 2 : 3; };
     const int sms = std::max(2, device_sm_count());
     for (Item& it : items) {
@@ -2050,7 +2127,7 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     if (st == kOk && plan.bimg_bytes) st = ws.bimg.reserve(plan.bimg_bytes);
     if (st == kOk && plan.coef_bytes) st = ws.coef.reserve(plan.coef_bytes);
     if (st == kOk && plan.sorted_bytes) st = ws.sorted.reserve(plan.sorted_bytes);
-    if (st == kOk) st = ws.slots.reserve(std::max<size_t>(plan.slot_floats * sizeof(float), 256));
+    if (st == kOk) st = ws.slots.reserve(std::max<size_t>(plan.slot_bytes, 256));
     if (st != kOk) return st;
     char* tp_base = static_cast<char*>(ws.particles.ptr);
     for (size_t j = 0; j < plan.jobs.size(); ++j) {
@@ -2058,7 +2135,7 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
         job.bimg = plan.bimg_offset[j] == SIZE_MAX ? nullptr
                                                    : static_cast<const unsigned char*>(ws.bimg.ptr) + plan.bimg_offset[j];
         job.blocks = reinterpret_cast<const unsigned char*>(tp_base + plan.job_tp[j]);
-        job.slots = static_cast<float*>(ws.slots.ptr) + plan.job_slot[j];
+        job.slots = static_cast<char*>(ws.slots.ptr) + plan.job_slot[j];
         job.colmap = reinterpret_cast<const int4*>(static_cast<char*>(ws.meta.ptr) + plan.colmap_offset) +
                      plan.job_colmap[j];
         job.coef = plan.job_coef[j] == SIZE_MAX ? nullptr : static_cast<const float*>(ws.coef.ptr) + plan.job_coef[j];
@@ -2116,6 +2193,57 @@ int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t st
     return kOk;
 }
 
+int tensor_prepare(const std::vector<SumRequest>& groups, TensorWorkspace& ws, cudaStream_t stream,
+                   const TensorPlan** plan) {
+    // everything tensor_plan reads, field by field (no padding bytes)
+    std::string key;
+    auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
+    int dev = -1;
+    cudaGetDevice(&dev);
+    put(&dev, sizeof dev);
+    const TuneParams& tp = active_tune();
+    const int tune[5] = {tp.plain_waves, tp.tc_waves, tp.tc_flush, tp.hbin_job_cost, tp.hbin_block_cost};
+    put(tune, sizeof tune);
+    const size_t limit = operand_cache_limit();
+    put(&limit, sizeof limit);
+    for (const SumRequest& r : groups) {
+        const void* ptrs[6] = {r.particles, r.radii, r.out, r.hbins, r.shell_edges, r.shell_first};
+        put(ptrs, sizeof ptrs);
+        const unsigned long long hid = r.hbins ? r.hbins->id : 0ull;
+        put(&hid, sizeof hid);
+        const float f[3] = {r.radius_min, r.radius_max, r.weight_max};
+        put(f, sizeof f);
+        const long long ll[4] = {r.out_base, r.out_sx, r.out_sy, r.out_sz};
+        put(ll, sizeof ll);
+        const int in[10] = {r.n, r.basis, r.wrap, r.row, r.accumulate ? 1 : 0, r.kink, r.shell_nbins,
+                            r.lat.nx, r.lat.ny, r.lat.nz};
+        put(in, sizeof in);
+        const int org[3] = {r.lat.x0, r.lat.y0, r.lat.z0};
+        put(org, sizeof org);
+        const double d[13] = {r.lat.kx, r.lat.ky, r.lat.kz, r.lat.m[0], r.lat.m[1], r.lat.m[2], r.lat.m[3],
+                              r.lat.m[4], r.lat.m[5], r.lat.m[6], r.lat.m[7], r.lat.m[8], r.scale};
+        put(d, sizeof d);
+        put(&r.stream, sizeof r.stream);
+        put(&r.error_flag, sizeof r.error_flag);
+    }
+    if (ws.plan && ws.plan_key == key) {
+        *plan = ws.plan.get();
+        return kOk;
+    }
+    ws.plan_key.clear();
+    auto fresh = std::make_unique<TensorPlan>();
+    int st = tensor_plan(groups, *fresh);
+    if (st == kOk) st = tensor_reserve_upload(*fresh, ws, stream);
+    if (st != kOk) {
+        ws.plan.reset();
+        return st;
+    }
+    ws.plan = std::move(fresh);
+    ws.plan_key = std::move(key);
+    *plan = ws.plan.get();
+    return kOk;
+}
+
 namespace {
 
 // One persistent launch of a tile mode: min(items, SMs) CTAs, or for the CTA
@@ -2170,7 +2298,7 @@ int reduce_smem(void (*kernel)(TcReduceArgs), size_t bytes) {
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag) {
     int st = kOk;
-    // zero the FP64 accumulators
+    // zero the per-compute counters (h-bin scatter cursors)
     if (plan.acc_bytes)
         st = check_cuda(cudaMemsetAsync(ws.acc.ptr, 0, plan.acc_bytes, stream), "cudaMemsetAsync(acc)");
     if (st != kOk) return st;
