@@ -120,8 +120,8 @@ void vis_autotune_clear(void);
  * factors of every particle, computed once per compute and copied by each
  * m-tile instead of recomputed).  A job whose images would exceed what is left
  * of the limit computes its B operands per tile instead (same results).
- * bytes < 0 restores the default: MV_TC_OPERAND_CACHE_MB if set, else an
- * eighth of the device's memory; 0 turns the images off.  The images take 16
+ * bytes < 0 restores the default: MV_TC_OPERAND_CACHE_MB if set, else three
+ * eighths of the device's memory; 0 turns the images off.  The images take 16
  * bytes per particle and tensor plane (2 GB for 2^20 particles on 256^3).
  * Process-wide; applies to later computes.  No counterpart in the reference. */
 void vis_set_operand_cache_limit(long long bytes);

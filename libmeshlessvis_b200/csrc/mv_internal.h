@@ -339,8 +339,8 @@ struct TensorWorkspace {
 int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan);
 
 // Device memory the B-operand images of one plan may take: the limit set with
-// vis_set_operand_cache_limit (or MV_TC_OPERAND_CACHE_MB), by default an
-// eighth of the current device's memory.
+// vis_set_operand_cache_limit (or MV_TC_OPERAND_CACHE_MB), by default three
+// eighths of the current device's memory.
 size_t operand_cache_limit();
 int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream);
 // tensor_plan + tensor_reserve_upload, skipped when the groups, the launch
