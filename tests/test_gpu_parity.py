@@ -98,6 +98,24 @@ def test_decaying_gaussian_many_groups_large_n_random_points():
     assert O.rel_l2(got, ref) < SPEC_TOL
 
 
+@pytest.mark.parametrize("grid,basis", [((32, 32, 32), M.WENDLAND_D3_C2), ((32, 32, 32), M.GAUSSIAN_DECAYING),
+                                        ((48, 32, 16), M.SPH), ((32, 48, 24), M.GAUSSIAN_DECAYING),
+                                        ((64, 64, 8), M.SPH)])
+def test_plain_form_whole_spectra_on_square_and_oblong_lattices(grid, basis):
+    """The plain (folded) form over whole half-spectra with per-particle radii
+    (Phi^ table and Gaussian exp2 amplitudes), on lattices whose x and y
+    extents agree and on oblong ones, against the FP64 sum at every point (the
+    reference's per-term sum, meshless_vis/fourier_transform.cu:100-130)."""
+    rng = np.random.default_rng(sum(grid) + basis)
+    n = 3001
+    h = np.exp(rng.uniform(np.log(0.01), np.log(0.06), n)).astype(np.float32)
+    groups = [(constraints(rng.random((n, 3)), rng.standard_normal(n)), h, basis)]
+    spec, _ = spectrum_and_views(groups, grid, 1.0, (1.0, 1.0), (grid[0] // 2, grid[1] // 2), grid[:2], None,
+                                 M.FORM_PLAIN)
+    ref = O.spectrum_grid(groups, 1.0, grid)
+    assert O.rel_l2(spec, ref) < SPEC_TOL
+
+
 def test_spectrum_l0_plane_is_hermitian():
     rng = np.random.default_rng(4)
     groups = [(constraints(rng.random((999, 3)), rng.standard_normal(999)), np.full(999, 0.03, np.float32), M.SPH)]
