@@ -227,6 +227,15 @@ struct TcJob {
     // the slot column of job column c (tc_reduce_kernel): (n-tile, Re column,
     // Im column, 0) per column
     const int4* colmap;
+    // Row-folded jobs (fold = F > 1; separable groups without per-particle
+    // Gaussian factors, whose terms are pure phases): the spectrum's b axis
+    // is split as b = F bh + bl + b_base, job rows (a, bh) (ky = Ky / F of
+    // them per a) and job columns bl * period + c_idx (period = the planes).
+    // The A operand carries the phase of F bh + b_base, B that of bl and c,
+    // so F planes' worth of columns share every A row: more columns per MMA
+    // (N = 256 instead of 64 or 128 on small lattices) and less A work per
+    // term.  0 or 1: no fold.
+    int fold;
 };
 
 // The h-bins of one binned group on one lattice (tensor_plan): consecutive

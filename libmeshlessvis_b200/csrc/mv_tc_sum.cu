@@ -214,7 +214,8 @@ struct TcItem {
     int bc0, bnc;  // the c values whose B rows this CTA produces: all of them, or one half (kPair)
     int row0;      // this CTA's first lattice row
     int a_base, b_base, c_base;  // the job's frequency offsets, in registers for the stage loops
-    int period;                  // h-binned job: frequency columns per Chebyshev block (else 0)
+    int period;                  // h-binned or row-folded job: frequency columns per column block (else 0)
+    int fold;                    // row-folded job: b steps per row (TcJob::fold), else 1
     const unsigned char* bimg;   // this CTA's B-operand images of the item's n-tile (one per block), or null
     int img_stride, img_bytes;   // bytes between images; bytes of one image (512 bnc)
     void* slot;                  // this CTA's part of the item's slot (TcJob::slots)
@@ -244,6 +245,7 @@ __device__ __forceinline__ TcItem tc_item(const TcArgs& a, int it, int rank) {
     r.b_base = r.job->b_base;
     r.c_base = r.job->c_base;
     r.period = r.job->period;
+    r.fold = r.job->fold > 1 ? r.job->fold : 1;
     r.img_stride = r.job->img_stride;
     r.img_bytes = 4 * r.bnc * kRowBytes;
     r.bimg = r.job->bimg ? r.job->bimg + (size_t)(r.n_tile * Shape<MODE>::kCtas + rank) * r.job->n_blocks *
@@ -573,23 +575,27 @@ __device__ __forceinline__ float chebyshev_t(int q, float t) {
 // at bhi: rows chunk*8 .. +7 of its Re F half and of its Im F half, hi rows
 // then lo rows 2 bnc rows later.  Column c_col is frequency c_col + c_base; in
 // an h-binned job (period > 0) it is frequency c_col % period + c_base of
-// Chebyshev block q = c_col / period, weighted by T_q(t).  The chain's 8
+// Chebyshev block q = c_col / period, weighted by T_q(t); in a row-folded job
+// (fold) block q = c_col / period is the b offset bl = q, whose phase q Qy
+// (fixed-point y turns pqy) joins the chain's start.  The chain's 8
 // frequencies c_s .. c_s + 7 rise from c_s >= 0 and never cross a block (the
 // period is a multiple of 8).  The producer warps run it into the stage
 // buffer and tc_bimg_kernel into global memory: one arithmetic for both.
 __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col, int c_col, int c_base, int period,
-                                       const uint32_t* pqz, const float* pgam, bool gauss, float2 RX, float2 RY,
-                                       float2 NRY, float2 RHO) {
+                                       bool fold, const uint32_t* pqz, const uint32_t* pqy, const float* pgam,
+                                       bool gauss, float2 RX, float2 RY, float2 NRY, float2 RHO) {
     int c_s = c_col + c_base, cheb = -1;
     if (period > 0) {
         cheb = c_col / period;
         c_s = c_col - cheb * period + c_base;
     }
+    const uint32_t bl = fold ? (uint32_t)cheb : 0u;
+    if (fold) cheb = -1;
     float v[2][3];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         float sn, cs;
-        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e]), &sn, &cs);
+        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e] + bl * pqy[e]), &sn, &cs);
         float g = kOperandScale, q = 1.f;
         if (gauss) {
             g *= exp2f(pgam[e] * (float)(c_s * c_s));
@@ -924,9 +930,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
             const bool gauss = I.job->gauss != 0;
             const int rho0 = I.row0 + rc * 8;
             const int a_x = rho0 / ky + I.a_base;
-            const int b0 = rho0 % ky + I.b_base;
+            // the chunk's 8 rows have b = b0, b0 + fold, ..., b0 + 7 fold (the
+            // constants' y rotation is the one of fold steps)
+            const int b0 = (rho0 % ky) * I.fold + I.b_base;
             const bool a_up = b0 >= 0;
-            const int b_s = a_up ? b0 : b0 + 7;
+            const int b_s = a_up ? b0 : b0 + 7 * I.fold;
             for (int s = 0; s < I.n_stages; ++s, ++S) {
                 const int buf = S % kSlots;
                 if (!__all_sync(0xffffffffu, mbar_wait(&pdata[buf], (S / kSlots) & 1, abort_flag, a.error_flag, a.wait_limit_ns, 64)))
@@ -960,12 +968,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                         prz[0] = prz[1] = make_float2(1.f, 0.f);
                     } else {
                         const uint2 zq = *reinterpret_cast<const uint2*>(blk + kOffQz + 8 * pp);
+                        const uint2 yq = *reinterpret_cast<const uint2*>(blk + kOffQy + 8 * pp);
                         const float4 r = *reinterpret_cast<const float4*>(blk + kOffRz + 16 * pp);
                         pqz[0] = zq.x;
                         pqz[1] = zq.y;
                         prz[0] = make_float2(r.x, r.y);
                         prz[1] = make_float2(r.z, r.w);
-                        pqx[0] = pqx[1] = pqy[0] = pqy[1] = 0u;
+                        pqy[0] = yq.x;  // row-folded jobs: the phase of a column block's b offset
+                        pqy[1] = yq.y;
+                        pqx[0] = pqx[1] = 0u;
                         pamp[0] = pamp[1] = 0.f;
                         pry[0] = pry[1] = make_float2(1.f, 0.f);
                     }
@@ -1032,7 +1043,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.bnc || I.bimg) break;  // the loader copies B images
-                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8, I.c_base, I.period, pqz, pgam, gauss, RX, RY,
+                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8, I.c_base, I.period, I.fold > 1, pqz, pqy, pgam,
+                               gauss, RX, RY,
                                NRY, RHO);
                     }
                 }
@@ -1095,6 +1107,7 @@ struct TcPrepArgs {
     float gamma_scale;
     float inv_wmax;
     bool gauss;
+    int fold;          // the planes' job's row fold (1: none): its y rotation covers fold steps
     uint8_t* out;      // ceil(n / 32) blocks
     uint8_t* out_nyq;  // the same with x and z exchanged (the Nyquist-plane job's), or null
 };
@@ -1125,7 +1138,7 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
     reinterpret_cast<float*>(blk + kOffGam)[l] = gam;
     reinterpret_cast<float*>(blk + kOffRho2)[l] = exp2f(2.f * gam);
     const float2 ry = unit_phase(qy);
-    reinterpret_cast<float2*>(blk + kOffRy)[l] = ry;
+    reinterpret_cast<float2*>(blk + kOffRy)[l] = p.fold > 1 ? unit_phase((uint32_t)p.fold * qy) : ry;
     reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(qz);
     if (p.out_nyq) {
         uint8_t* t = p.out_nyq + (size_t)(j / kBlockParticles) * kBlockBytes;
@@ -1297,18 +1310,19 @@ __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
     if (chunk * 8 >= bnc) return;
     const unsigned char* blk = J.blocks + (size_t)block * kBlockBytes;
     const uint2 zq = *reinterpret_cast<const uint2*>(blk + kOffQz + 8 * pp);
+    const uint2 yq = *reinterpret_cast<const uint2*>(blk + kOffQy + 8 * pp);
     const uint2 gq = *reinterpret_cast<const uint2*>(blk + kOffGam + 8 * pp);
     const uint2 rq = *reinterpret_cast<const uint2*>(blk + kOffRho2 + 8 * pp);
     const float4 r = *reinterpret_cast<const float4*>(blk + kOffRz + 16 * pp);
-    const uint32_t pqz[2] = {zq.x, zq.y};
+    const uint32_t pqz[2] = {zq.x, zq.y}, pqy[2] = {yq.x, yq.y};
     const float pgam[2] = {__uint_as_float(gq.x), __uint_as_float(gq.y)};
     const float2 RX = make_float2(r.x, r.z), RY = make_float2(r.y, r.w);
     const float2 NRY = make_float2(-RY.x, -RY.y);
     const bool gauss = J.gauss != 0;
     const float2 RHO = gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
     uint8_t* out = const_cast<uint8_t*>(J.bimg) + (size_t)img * J.img_stride;
-    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, J.c_base, J.period, pqz, pgam, gauss, RX, RY, NRY,
-           RHO);
+    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, J.c_base, J.period, J.fold > 1, pqz, pqy, pgam, gauss,
+           RX, RY, NRY, RHO);
 }
 
 // What the reduction needs of a job, gathered into shared memory once per
@@ -1323,6 +1337,7 @@ struct ReduceJob {
     int rank_stride;    // floats between the CTAs' parts of a slot: 128 * 2 nc_tile
     int mrows_log2;     // 7 (one CTA) or 8 (CTA pair)
     int period, blocks, coef_stride;
+    int fold, ky_full;  // row-folded jobs: the fold and the spectrum's Ky (else 1, 0)
 };
 
 __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
@@ -1330,7 +1345,7 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     r.slots = J.slots;
     r.slot_fp64 = J.slot_fp64;
     r.colmap = J.colmap;
-    r.coef = J.period > 0 ? J.coef : nullptr;
+    r.coef = J.period > 0 && J.fold <= 1 ? J.coef : nullptr;
     r.scale = J.wmax * kInvProductScale;
     r.slot_stride = J.slot_stride;
     r.n_splits = J.n_splits;
@@ -1341,18 +1356,29 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     r.period = J.period;
     r.blocks = J.period > 0 ? J.lz_tc / J.period : 1;
     r.coef_stride = J.coef_stride;
+    r.fold = J.fold > 1 ? J.fold : 1;
+    r.ky_full = J.ky * r.fold;
     return r;
 }
 
-// Adds one job's contribution at lattice row rho (within the job's rows) and
-// the kC consecutive frequency columns c0 .. c0 + kC - 1 (c_idx, before the
-// Chebyshev blocks of an h-binned job; they share one n-tile and one CTA half,
-// as n-tiles and halves hold multiples of 8 columns): the totals of all its
-// particle chunks (FP32 or FP64 slots) summed in FP64, each h-binned block
-// weighted by its coefficient at |k|^2 = n2[i] step^2, times W 2^-24.
+// Adds one job's contribution at lattice row rho (the spectrum's a_idx Ky +
+// b_idx; within the job's rows for unfolded jobs) and the kC consecutive
+// frequency columns c0 .. c0 + kC - 1 (c_idx, before the Chebyshev blocks of
+// an h-binned job; they share one n-tile and one CTA half, as n-tiles and
+// halves hold multiples of 8 columns): the totals of all its particle chunks
+// (FP32 or FP64 slots) summed in FP64, each h-binned block weighted by its
+// coefficient at |k|^2 = n2[i] step^2, times W 2^-24.  A row-folded job holds
+// b_idx = fold bh + bl at job row a_idx (Ky / fold) + bh, column block bl.
 constexpr int kReduceC = 4;
 __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, const int* n2, int nc, double* sr,
                                            double* si, double sign_im) {
+    int q_first = 0, q_end = J.blocks;
+    if (J.fold > 1) {
+        const int a_idx = rho / J.ky_full, b_idx = rho - a_idx * J.ky_full;
+        rho = a_idx * (J.ky_full / J.fold) + b_idx / J.fold;
+        q_first = b_idx % J.fold;
+        q_end = q_first + 1;
+    }
     const int m_tile = rho >> J.mrows_log2, within = rho - (m_tile << J.mrows_log2);
     const int rank = within >> 7, rl = within & (kM - 1);
     // FP32 slot layout [column / 4][128 rows][column % 4]: column n of row rl
@@ -1361,7 +1387,7 @@ __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, 
     const size_t rbase = (size_t)rank * J.rank_stride;
     const float* row = static_cast<const float*>(J.slots) + rbase + rl * 4;
     const double* row64 = static_cast<const double*>(J.slots) + rbase + rl * 2;
-    for (int q = 0; q < J.blocks; ++q) {
+    for (int q = q_first; q < q_end; ++q) {
         const int4 m = __ldg(J.colmap + q * J.period + c0);  // the same for a warp's rows
         double tr[kReduceC] = {}, ti[kReduceC] = {};
         for (int ks = 0; ks < J.n_splits; ++ks) {
@@ -1523,6 +1549,15 @@ bool is_spectrum_lattice(const Lattice& L) {
     if (!(s > 0) || L.ky != s || L.kz != s) return false;
     return L.m[0] == s && L.m[4] == s && L.m[8] == s && L.m[1] == 0 && L.m[2] == 0 && L.m[3] == 0 && L.m[5] == 0 &&
            L.m[6] == 0 && L.m[7] == 0;
+}
+
+// Row folds of pure-phase groups: MV_TC_FOLD=0 turns them off.
+bool tc_fold_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("MV_TC_FOLD");
+        return !(e && e[0] == '0');
+    }();
+    return v;
 }
 
 // kPair tiles: MV_TC_PAIRS=0 turns them off (jobs then take kWide tiles).
@@ -2027,17 +2062,34 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             (size_t)((std::max(0, r.n) + kBlockParticles - 1) / kBlockParticles) * kBlockBytes;
         plan.tp_bytes += blocks_bytes;
         const int mode = mode_of(lz_tc, (long long)kx * ky);
+        // Row fold of a group whose terms are pure phases: the F of {1, 2, 4}
+        // whose columns F lz_tc fill the MMAs best.  A CTA-pair (or narrow)
+        // MMA costs about the same whatever its N up to 256 (128 c values),
+        // so the cost per column is n-tiles / columns.
+        int fold = 1;
+        if (!gauss && tc_fold_enabled()) {
+            auto cost = [&](int f) {
+                const int cols = f * lz_tc;
+                const int nc_max = cols <= Shape<kNarrow>::kNc ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
+                return (double)((cols + nc_max - 1) / nc_max) / cols;
+            };
+            for (int f : {2, 4})
+                if (ky % (16 * f) == 0 && cost(f) < cost(fold) * 0.99) fold = f;
+        }
         TcJob j{};
         j.kx = kx;
-        j.ky = ky;
-        j.lz_tc = lz_tc;
+        j.ky = ky / fold;
+        j.lz_tc = fold * lz_tc;
         j.a_base = -kx / 2;
         j.b_base = -ky / 2;
         j.c_base = 0;
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
-        plan.job_of_group.push_back(add_job(j, mode, true, plan.tp_offset.back(), cls, 0, SIZE_MAX));
+        j.fold = fold;
+        j.period = fold > 1 ? lz_tc : 0;
+        plan.job_of_group.push_back(add_job(j, mode_of(j.lz_tc, (long long)kx * j.ky), true, plan.tp_offset.back(),
+                                            cls, 0, SIZE_MAX));
         // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
         // -a > 0; see TcJob) in the same launch, where the Kx / 2 columns of
         // each split into whole n-tile units (16 c for kPair, else 8);
@@ -2053,6 +2105,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             t.a_base = lz_tc;
             t.b_base = -ky / 2;
             t.c_base = 0;
+            t.fold = 0;
+            t.period = 0;
             const size_t tpn = plan.tp_nyq_offset.back();
             plan.nyq_job_of_group.back() = add_job(t, mode, false, tpn, cls, 1, SIZE_MAX);  // one m-tile: no reuse
             t.a_base = -lz_tc;
@@ -2371,6 +2425,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         pa.gauss = plan.jobs[j].gauss != 0;
         pa.gamma_scale = pa.gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
         pa.inv_wmax = 1.0f / r.weight_max;
+        pa.fold = std::max(1, plan.jobs[j].fold);
         pa.out = const_cast<unsigned char*>(plan.jobs[j].blocks);
         const int t = plan.nyq_job_of_group[g];
         pa.out_nyq = t < 0 ? nullptr : const_cast<unsigned char*>(plan.jobs[t].blocks);
