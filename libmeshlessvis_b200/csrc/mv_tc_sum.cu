@@ -575,22 +575,24 @@ __device__ __forceinline__ float chebyshev_t(int q, float t) {
 // at bhi: rows chunk*8 .. +7 of its Re F half and of its Im F half, hi rows
 // then lo rows 2 bnc rows later.  Column c_col is frequency c_col + c_base; in
 // an h-binned job (period > 0) it is frequency c_col % period + c_base of
-// Chebyshev block q = c_col / period, weighted by T_q(t); in a row-folded job
-// (fold) block q = c_col / period is the b offset bl = q, whose phase q Qy
-// (fixed-point y turns pqy) joins the chain's start.  The chain's 8
+// column block k = c_col / period: in a row-folded job (fold = F > 1) the b
+// offset bl = k mod F, whose phase bl Qy (fixed-point y turns pqy) joins the
+// chain's start; in an h-binned job (cheb_blocks) Chebyshev block q = k / F,
+// weighted by T_q(t).  The chain's 8
 // frequencies c_s .. c_s + 7 rise from c_s >= 0 and never cross a block (the
 // period is a multiple of 8).  The producer warps run it into the stage
 // buffer and tc_bimg_kernel into global memory: one arithmetic for both.
 __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col, int c_col, int c_base, int period,
-                                       bool fold, const uint32_t* pqz, const uint32_t* pqy, const float* pgam,
-                                       bool gauss, float2 RX, float2 RY, float2 NRY, float2 RHO) {
+                                       int fold, bool cheb_blocks, const uint32_t* pqz, const uint32_t* pqy,
+                                       const float* pgam, bool gauss, float2 RX, float2 RY, float2 NRY, float2 RHO) {
     int c_s = c_col + c_base, cheb = -1;
+    uint32_t bl = 0u;
     if (period > 0) {
-        cheb = c_col / period;
-        c_s = c_col - cheb * period + c_base;
+        const int blk = c_col / period;
+        c_s = c_col - blk * period + c_base;
+        bl = (uint32_t)(blk % fold);
+        if (cheb_blocks) cheb = blk / fold;
     }
-    const uint32_t bl = fold ? (uint32_t)cheb : 0u;
-    if (fold) cheb = -1;
     float v[2][3];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -1043,8 +1045,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                     for (int h = 0; h < SH::kChunksPerThread; ++h) {
                         const int chunk = cb + 8 * h;
                         if (chunk * 8 >= I.bnc || I.bimg) break;  // the loader copies B images
-                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8, I.c_base, I.period, I.fold > 1, pqz, pqy, pgam,
-                               gauss, RX, RY,
+                        b_unit(bhi, I.bnc, chunk, col, I.bc0 + chunk * 8, I.c_base, I.period, I.fold,
+                               I.job->coef != nullptr, pqz, pqy, pgam, gauss, RX, RY,
                                NRY, RHO);
                     }
                 }
@@ -1186,6 +1188,7 @@ struct TcBinnedPrepArgs {
     float4* sorted;        // particles sorted by bin (for the branch part)
     float* sorted_radii;
     int* error_flag;
+    int fold;              // the bins' planes jobs' row fold (1: none): their y rotation covers fold steps
 };
 
 // Scatters each particle's constants into its bin's blocks (order within a
@@ -1214,6 +1217,7 @@ __global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
     const size_t blk_off = (size_t)(bin.x + slot / kBlockParticles) * kBlockBytes;
     const int l = slot % kBlockParticles;
     const float2 ry = unit_phase(qy);
+    const float2 ry_fold = p.fold > 1 ? unit_phase((uint32_t)p.fold * qy) : ry;
     for (int pass = 0; pass < (p.out_nyq ? 2 : 1); ++pass) {
         uint8_t* blk = (pass == 0 ? p.out : p.out_nyq) + blk_off;
         const uint32_t ax = pass == 0 ? qx : qz, az = pass == 0 ? qz : qx;
@@ -1223,7 +1227,7 @@ __global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
         reinterpret_cast<float*>(blk + kOffAmp)[l] = amp;
         reinterpret_cast<float*>(blk + kOffGam)[l] = t;
         reinterpret_cast<float*>(blk + kOffRho2)[l] = 1.f;
-        reinterpret_cast<float2*>(blk + kOffRy)[l] = ry;
+        reinterpret_cast<float2*>(blk + kOffRy)[l] = pass == 0 ? ry_fold : ry;
         reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(az);
     }
 }
@@ -1321,8 +1325,8 @@ __global__ void __launch_bounds__(256) tc_bimg_kernel(TcImageArgs g) {
     const bool gauss = J.gauss != 0;
     const float2 RHO = gauss ? make_float2(__uint_as_float(rq.x), __uint_as_float(rq.y)) : make_float2(1.f, 1.f);
     uint8_t* out = const_cast<uint8_t*>(J.bimg) + (size_t)img * J.img_stride;
-    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, J.c_base, J.period, J.fold > 1, pqz, pqy, pgam, gauss,
-           RX, RY, NRY, RHO);
+    b_unit(out, bnc, chunk, 8 * pp, c0 + half * bnc + chunk * 8, J.c_base, J.period, max(1, J.fold), J.coef != nullptr,
+           pqz, pqy, pgam, gauss, RX, RY, NRY, RHO);
 }
 
 // What the reduction needs of a job, gathered into shared memory once per
@@ -1345,7 +1349,7 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     r.slots = J.slots;
     r.slot_fp64 = J.slot_fp64;
     r.colmap = J.colmap;
-    r.coef = J.period > 0 && J.fold <= 1 ? J.coef : nullptr;
+    r.coef = J.period > 0 ? J.coef : nullptr;
     r.scale = J.wmax * kInvProductScale;
     r.slot_stride = J.slot_stride;
     r.n_splits = J.n_splits;
@@ -1354,7 +1358,7 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     r.rank_stride = kM * 2 * J.nc_tile;
     r.mrows_log2 = J.ctas == 2 ? 8 : 7;
     r.period = J.period;
-    r.blocks = J.period > 0 ? J.lz_tc / J.period : 1;
+    r.blocks = J.period > 0 ? J.lz_tc / J.period / (J.fold > 1 ? J.fold : 1) : 1;
     r.coef_stride = J.coef_stride;
     r.fold = J.fold > 1 ? J.fold : 1;
     r.ky_full = J.ky * r.fold;
@@ -1368,16 +1372,16 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
 // halves hold multiples of 8 columns): the totals of all its particle chunks
 // (FP32 or FP64 slots) summed in FP64, each h-binned block weighted by its
 // coefficient at |k|^2 = n2[i] step^2, times W 2^-24.  A row-folded job holds
-// b_idx = fold bh + bl at job row a_idx (Ky / fold) + bh, column block bl.
+// b_idx = fold bh + bl at job row a_idx (Ky / fold) + bh, in column blocks
+// q fold + bl.
 constexpr int kReduceC = 4;
 __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, const int* n2, int nc, double* sr,
                                            double* si, double sign_im) {
-    int q_first = 0, q_end = J.blocks;
+    int bl = 0;
     if (J.fold > 1) {
         const int a_idx = rho / J.ky_full, b_idx = rho - a_idx * J.ky_full;
         rho = a_idx * (J.ky_full / J.fold) + b_idx / J.fold;
-        q_first = b_idx % J.fold;
-        q_end = q_first + 1;
+        bl = b_idx % J.fold;
     }
     const int m_tile = rho >> J.mrows_log2, within = rho - (m_tile << J.mrows_log2);
     const int rank = within >> 7, rl = within & (kM - 1);
@@ -1387,8 +1391,9 @@ __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, 
     const size_t rbase = (size_t)rank * J.rank_stride;
     const float* row = static_cast<const float*>(J.slots) + rbase + rl * 4;
     const double* row64 = static_cast<const double*>(J.slots) + rbase + rl * 2;
-    for (int q = q_first; q < q_end; ++q) {
-        const int4 m = __ldg(J.colmap + q * J.period + c0);  // the same for a warp's rows
+    for (int q = 0; q < J.blocks; ++q) {
+        // column block q F + bl: Chebyshev block q (h-binned), b offset bl (folded)
+        const int4 m = __ldg(J.colmap + (q * J.fold + bl) * J.period + c0);  // the same for a warp's rows
         double tr[kReduceC] = {}, ti[kReduceC] = {};
         for (int ks = 0; ks < J.n_splits; ++ks) {
             const size_t li = ((size_t)ks * J.n_mtiles + m_tile) * J.n_ntiles + m.x;
@@ -1673,11 +1678,23 @@ long long lattice_nsq(const Lattice& L) {
 }
 
 // Work per particle of a bin of Chebyshev order P whose blocks are `period`
-// columns wide: the A operand is produced once per n-tile (at most 128 c
-// values), the MMAs scale with the columns; both in units of one full n-tile.
-double hbin_unit_cost(int order, int period) {
+// columns wide, in jobs folded by `fold` rows: the MMAs cost about the same
+// per n-tile (at most 128 c values) whatever its width, and a fold puts
+// `fold` rows' columns into one job row (1 / fold of the m-tiles); the A and
+// B operands' work scales with the columns; in units of one full n-tile.
+double hbin_unit_cost(int order, int period, int fold) {
     const double tiles = (double)order * period / Shape<kWide>::kNc;
-    return std::ceil(tiles) + tiles;
+    return std::ceil(tiles * fold) / fold + tiles;
+}
+
+// Row fold of an h-binned group's plane jobs (TcJob::fold): the smallest F of
+// {1, 2, 4} whose F planes fill whole n-tiles for every Chebyshev order, if
+// Ky / F stays a multiple of 16; else 1.
+int hbin_fold(const Lattice& L) {
+    const int period = L.nz - 1;
+    for (int f : {1, 2, 4})
+        if ((f * period) % Shape<kWide>::kNc == 0 && L.ny % (16 * f) == 0) return f > 1 && !tc_fold_enabled() ? 1 : f;
+    return 1;
 }
 
 // Bins of a group on a lattice: runs of fine bins chosen by dynamic
@@ -1685,7 +1702,7 @@ double hbin_unit_cost(int order, int period) {
 // tensor work) + order x block_cost (the reduction reads every Chebyshev
 // block at every frequency) + job_cost (items, pipeline fills), each bin's
 // Chebyshev interval the span of its non-empty fine bins.
-HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_cost, int block_cost) {
+HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int fold, int job_cost, int block_cost) {
     const int F = kHBinFine;
     std::vector<long long> cum(F + 1, 0);
     for (int f = 0; f < F; ++f) cum[f + 1] = cum[f] + hs.count[f];
@@ -1705,7 +1722,7 @@ HBinPlan hbin_plan_build(const HBinStats& hs, double kmax, int period, int job_c
                 if (order > kHBinMaxOrder) break;  // wider runs (smaller i) only need more
             }
             const double c =
-                best[i] + (n > 0 ? (double)n * hbin_unit_cost(order, period) + (double)order * block_cost + job_cost : 0.0);
+                best[i] + (n > 0 ? (double)n * hbin_unit_cost(order, period, fold) + (double)order * block_cost + job_cost : 0.0);
             if (c < best[j]) {
                 best[j] = c;
                 arg[j] = i;
@@ -1764,13 +1781,14 @@ std::shared_ptr<const HBinPlan> hbin_plan(const SumRequest& r) {
     const int job_cost = env_job >= 0 ? env_job : std::max(0, active_tune().hbin_job_cost);
     const int block_cost = env_block >= 0 ? env_block : std::max(0, active_tune().hbin_block_cost);
     const int period = r.lat.nz - 1;
-    const auto key = std::make_tuple(r.hbins->id, (nsq * 65536 + period) * 4 + r.basis, r.lat.kx,
+    const int fold = hbin_fold(r.lat);
+    const auto key = std::make_tuple(r.hbins->id, ((nsq * 65536 + period) * 4 + r.basis) * 8 + fold, r.lat.kx,
                                      (long long)job_cost * 2000003LL + block_cost);
     std::lock_guard<std::mutex> lock(g_hbin_mu);
     auto it = g_hbin_cache.find(key);
     if (it != g_hbin_cache.end()) return it->second;
     if (g_hbin_cache.size() >= 256) g_hbin_cache.clear();
-    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, period, job_cost, block_cost));
+    auto plan = std::make_shared<const HBinPlan>(hbin_plan_build(*r.hbins, kmax, period, fold, job_cost, block_cost));
     g_hbin_cache[key] = plan;
     return plan;
 }
@@ -2012,6 +2030,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             }
             size_t coef_at = 0;
             int first_job = -1, first_nyq = -1;
+            const int bfold = hbin_fold(L);
             for (int b = 0; b < bg.nbins; ++b) {
                 const HBin& bin = bg.bins[b];
                 const size_t coef_off = bg.coef_offset + coef_at;  // the bin's first block, within one |k|^2
@@ -2019,8 +2038,8 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
                 if (bin.count <= 0 || !(bin.wmax > 0.f)) continue;
                 TcJob j{};
                 j.kx = kx;
-                j.ky = ky;
-                j.lz_tc = bin.order * lz_tc;
+                j.ky = ky / bfold;
+                j.lz_tc = bin.order * lz_tc * bfold;  // column blocks q bfold + bl of lz_tc planes
                 j.a_base = -kx / 2;
                 j.b_base = -ky / 2;
                 j.c_base = 0;
@@ -2028,9 +2047,10 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
                 j.gauss = 0;
                 j.wmax = bin.wmax;
                 j.period = lz_tc;
+                j.fold = bfold;
                 j.coef_stride = bg.total_q;
                 const size_t tp = plan.tp_offset.back() + (size_t)first_block[b] * kBlockBytes;
-                const int jm = add_job(j, mode_of(j.lz_tc, (long long)kx * ky), true, tp, cls, 0, coef_off);
+                const int jm = add_job(j, mode_of(j.lz_tc, (long long)kx * j.ky), true, tp, cls, 0, coef_off);
                 if (first_job < 0) first_job = jm;
                 if (nyq) {
                     TcJob t = j;
@@ -2038,6 +2058,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
                     t.ky = ky;
                     t.lz_tc = bin.order * (kx / 2);
                     t.period = kx / 2;
+                    t.fold = 0;
                     t.a_base = lz_tc;
                     t.b_base = -ky / 2;
                     t.c_base = 0;
@@ -2398,6 +2419,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             bp.sorted = reinterpret_cast<float4*>(sorted);
             bp.sorted_radii = reinterpret_cast<float*>(sorted + ((size_t)r.n * sizeof(float4) + 255) / 256 * 256);
             bp.error_flag = error_flag;
+            bp.fold = std::max(1, plan.jobs[j].fold);
             tc_prep_binned_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(bp);
             count_launch();
             TcCoefArgs ca;
