@@ -236,6 +236,14 @@ struct TcJob {
     // (N = 256 instead of 64 or 128 on small lattices) and less A work per
     // term.  0 or 1: no fold.
     int fold;
+    // Axis-exchanged jobs (exch = 1; groups whose amplitudes separate per
+    // axis, on lattices with more b values than tensor planes): rows (a,
+    // c_idx) with ky = the planes Kz/2 and b_base = 0, columns b_idx with
+    // lz_tc = Ky and c_base = -Ky/2 (B chains of negative b fall away from
+    // 0); the particle constants carry y and z exchanged.  192 planes with
+    // Ky = 384 then run 3 n-tiles of 128 b values (N = 256 MMAs) instead of
+    // two of 96 planes.
+    int exch;
 };
 
 // The h-bins of one binned group on one lattice (tensor_plan): consecutive

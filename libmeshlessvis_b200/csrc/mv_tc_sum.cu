@@ -533,7 +533,9 @@ __device__ __forceinline__ void a_chain(uint8_t* base, int c16, float2 X, float2
 
 // A B unit's 8 c values for its two particles: (Re B, -Im B) at re_base (a
 // Re F row), (Im B, Re B) at im_base (the Im F row); lo goes lo_gap after hi.
-template <bool GAUSS>
+// UP: the chain starts at the unit's first column and rises; otherwise it
+// starts at the last and falls (negative frequencies, moving away from 0).
+template <bool GAUSS, bool UP>
 __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int lo_gap, int c16, float2 X, float2 Y,
                                         float2 RX, float2 RY, float2 NRY, float2 Q, float2 RHO) {
     if constexpr (GAUSS) {  // the first step's ratio q0 = Q
@@ -543,7 +545,7 @@ __device__ __forceinline__ void b_chain(uint8_t* re_base, uint8_t* im_base, int 
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int off = sw_step(c16, i);
+        const int off = sw_step(c16, UP ? i : 7 - i);
         uint2 hi, lo;
         split_pair(X, Y, hi, lo);
         *reinterpret_cast<uint2*>(re_base + off) = make_uint2(h2_swap_negate(hi.x, true), h2_swap_negate(hi.y, true));
@@ -593,15 +595,19 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
         bl = (uint32_t)(blk % fold);
         if (cheb_blocks) cheb = blk / fold;
     }
+    // a unit of negative frequencies (the axis-exchanged jobs' b columns)
+    // starts at its top and falls
+    const bool down = c_s < 0;
+    const int c_t = down ? c_s + 7 : c_s;
     float v[2][3];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
         float sn, cs;
-        __sincosf(turns_to_radians((uint32_t)c_s * pqz[e] + bl * pqy[e]), &sn, &cs);
+        __sincosf(turns_to_radians((uint32_t)c_t * pqz[e] + bl * pqy[e]), &sn, &cs);
         float g = kOperandScale, q = 1.f;
         if (gauss) {
-            g *= exp2f(pgam[e] * (float)(c_s * c_s));
-            q = exp2f(pgam[e] * (float)(2 * c_s + 1));
+            g *= exp2f(pgam[e] * (float)(c_t * c_t));
+            q = exp2f(pgam[e] * (float)(down ? 1 - 2 * c_t : 2 * c_t + 1));
         } else if (cheb >= 0) {
             g *= chebyshev_t(cheb, pgam[e]);
         }
@@ -615,9 +621,15 @@ __device__ __forceinline__ void b_unit(uint8_t* bhi, int bnc, int chunk, int col
     uint8_t* re_base = bhi + chunk * 8 * kRowBytes + (col & 15);
     uint8_t* im_base = bhi + (bnc + chunk * 8) * kRowBytes + (col & 15);
     const int c16 = col & ~15;
-    if (gauss) b_chain<true>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY,
-                             make_float2(v[0][2], v[1][2]), RHO);
-    else b_chain<false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, make_float2(1.f, 1.f), RHO);
+    const float2 Q = gauss ? make_float2(v[0][2], v[1][2]) : make_float2(1.f, 1.f);
+    // falling: the conjugate rotation
+    if (down) {
+        if (gauss) b_chain<true, false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, NRY, RY, Q, RHO);
+        else b_chain<false, false>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, NRY, RY, Q, RHO);
+    } else {
+        if (gauss) b_chain<true, true>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
+        else b_chain<false, true>(re_base, im_base, 2 * bnc * kRowBytes, c16, X, Y, RX, RY, NRY, Q, RHO);
+    }
 }
 
 // Persistent: CTA (or CTA pair) b walks items b, b + grid, ... of the
@@ -1110,6 +1122,7 @@ struct TcPrepArgs {
     float inv_wmax;
     bool gauss;
     int fold;          // the planes' job's row fold (1: none): its y rotation covers fold steps
+    int exch;          // the planes' job is axis-exchanged: its blocks carry y and z exchanged
     uint8_t* out;      // ceil(n / 32) blocks
     uint8_t* out_nyq;  // the same with x and z exchanged (the Nyquist-plane job's), or null
 };
@@ -1133,15 +1146,16 @@ __global__ void tc_prep_kernel(TcPrepArgs p) {
             gam = p.gamma_scale * h * h;
         }
     }
+    const uint32_t by = p.exch ? qz : qy, bz = p.exch ? qy : qz;  // the planes job's row and column axes
     reinterpret_cast<uint32_t*>(blk + kOffQx)[l] = qx;
-    reinterpret_cast<uint32_t*>(blk + kOffQy)[l] = qy;
-    reinterpret_cast<uint32_t*>(blk + kOffQz)[l] = qz;
+    reinterpret_cast<uint32_t*>(blk + kOffQy)[l] = by;
+    reinterpret_cast<uint32_t*>(blk + kOffQz)[l] = bz;
     reinterpret_cast<float*>(blk + kOffAmp)[l] = amp;
     reinterpret_cast<float*>(blk + kOffGam)[l] = gam;
     reinterpret_cast<float*>(blk + kOffRho2)[l] = exp2f(2.f * gam);
     const float2 ry = unit_phase(qy);
-    reinterpret_cast<float2*>(blk + kOffRy)[l] = p.fold > 1 ? unit_phase((uint32_t)p.fold * qy) : ry;
-    reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(qz);
+    reinterpret_cast<float2*>(blk + kOffRy)[l] = unit_phase((uint32_t)p.fold * by);
+    reinterpret_cast<float2*>(blk + kOffRz)[l] = unit_phase(bz);
     if (p.out_nyq) {
         uint8_t* t = p.out_nyq + (size_t)(j / kBlockParticles) * kBlockBytes;
         reinterpret_cast<uint32_t*>(t + kOffQx)[l] = qz;
@@ -1342,6 +1356,7 @@ struct ReduceJob {
     int mrows_log2;     // 7 (one CTA) or 8 (CTA pair)
     int period, blocks, coef_stride;
     int fold, ky_full;  // row-folded jobs: the fold and the spectrum's Ky (else 1, 0)
+    int exch, rows_a;   // axis-exchanged jobs: 1 and the job rows per a (the planes)
 };
 
 __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
@@ -1361,7 +1376,9 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
     r.blocks = J.period > 0 ? J.lz_tc / J.period / (J.fold > 1 ? J.fold : 1) : 1;
     r.coef_stride = J.coef_stride;
     r.fold = J.fold > 1 ? J.fold : 1;
-    r.ky_full = J.ky * r.fold;
+    r.ky_full = J.exch ? J.lz_tc : J.ky * r.fold;
+    r.exch = J.exch;
+    r.rows_a = J.ky;
     return r;
 }
 
@@ -1377,6 +1394,35 @@ __device__ __forceinline__ ReduceJob reduce_job(const TcJob& J) {
 constexpr int kReduceC = 4;
 __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, const int* n2, int nc, double* sr,
                                            double* si, double sign_im) {
+    if (J.exch) {
+        // axis-exchanged: plane c0 + i of spectrum row (a_idx, b_idx) is job
+        // row a_idx (planes) + c0 + i, job column b_idx; the kC rows share a
+        // 128-row CTA half (c0 is a multiple of kC)
+        const int a_idx = rho / J.ky_full, b_idx = rho - a_idx * J.ky_full;
+        const int4 m = __ldg(J.colmap + b_idx);
+        for (int i = 0; i < nc; ++i) {
+            const int jr = a_idx * J.rows_a + c0 + i;
+            const int m_tile = jr >> J.mrows_log2, within = jr - (m_tile << J.mrows_log2);
+            const int rank = within >> 7, rl = within & (kM - 1);
+            double tr = 0.0, ti = 0.0;
+            for (int ks = 0; ks < J.n_splits; ++ks) {
+                const size_t li = ((size_t)ks * J.n_mtiles + m_tile) * J.n_ntiles + m.x;
+                const size_t base = li * J.slot_stride + (size_t)rank * J.rank_stride;
+                if (J.slot_fp64) {
+                    const double* v = static_cast<const double*>(J.slots) + base + rl * 2;
+                    tr += __ldg(v + (size_t)(m.y & ~1) * kM + (m.y & 1));
+                    ti += __ldg(v + (size_t)(m.z & ~1) * kM + (m.z & 1));
+                } else {
+                    const float* v = static_cast<const float*>(J.slots) + base + rl * 4;
+                    tr += (double)__ldg(v + (size_t)(m.y & ~3) * kM + (m.y & 3));
+                    ti += (double)__ldg(v + (size_t)(m.z & ~3) * kM + (m.z & 3));
+                }
+            }
+            sr[i] = fma(J.scale, tr, sr[i]);
+            si[i] = fma(J.scale * sign_im, ti, si[i]);
+        }
+        return;
+    }
     int bl = 0;
     if (J.fold > 1) {
         const int a_idx = rho / J.ky_full, b_idx = rho - a_idx * J.ky_full;
@@ -1560,6 +1606,15 @@ bool is_spectrum_lattice(const Lattice& L) {
 bool tc_fold_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("MV_TC_FOLD");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
+// Axis exchange of non-folding groups: MV_TC_EXCHANGE=0 turns it off.
+bool tc_exchange_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("MV_TC_EXCHANGE");
         return !(e && e[0] == '0');
     }();
     return v;
@@ -2097,18 +2152,31 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             for (int f : {2, 4})
                 if (ky % (16 * f) == 0 && cost(f) < cost(fold) * 0.99) fold = f;
         }
+        // Axis exchange of a group that cannot fold (per-particle Gaussian
+        // factors): rows (a, c), columns b, where Ky columns fill the MMAs
+        // better than the planes (384^3: 3 n-tiles of 128 b values instead of
+        // 96 + 96 planes)
+        bool exch = false;
+        if (fold == 1 && tc_exchange_enabled()) {
+            auto cost = [&](int cols) {
+                const int nc_max = cols <= Shape<kNarrow>::kNc ? Shape<kNarrow>::kNc : Shape<kWide>::kNc;
+                return (double)((cols + nc_max - 1) / nc_max) / cols;
+            };
+            exch = ky % 16 == 0 && ((long long)kx * lz_tc) % 256 == 0 && cost(ky) < cost(lz_tc) * 0.99;
+        }
         TcJob j{};
         j.kx = kx;
-        j.ky = ky / fold;
-        j.lz_tc = fold * lz_tc;
+        j.ky = exch ? lz_tc : ky / fold;
+        j.lz_tc = exch ? ky : fold * lz_tc;
         j.a_base = -kx / 2;
-        j.b_base = -ky / 2;
-        j.c_base = 0;
+        j.b_base = exch ? 0 : -ky / 2;
+        j.c_base = exch ? -ky / 2 : 0;
         j.n = r.n;
         j.gauss = gauss ? 1 : 0;
         j.wmax = r.weight_max;
         j.fold = fold;
         j.period = fold > 1 ? lz_tc : 0;
+        j.exch = exch ? 1 : 0;
         plan.job_of_group.push_back(add_job(j, mode_of(j.lz_tc, (long long)kx * j.ky), true, plan.tp_offset.back(),
                                             cls, 0, SIZE_MAX));
         // The Nyquist plane as two transposed jobs (rows b, columns a >= 0 and
@@ -2128,6 +2196,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             t.c_base = 0;
             t.fold = 0;
             t.period = 0;
+            t.exch = 0;
             const size_t tpn = plan.tp_nyq_offset.back();
             plan.nyq_job_of_group.back() = add_job(t, mode, false, tpn, cls, 1, SIZE_MAX);  // one m-tile: no reuse
             t.a_base = -lz_tc;
@@ -2448,6 +2517,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         pa.gamma_scale = pa.gauss ? (float)(-(double)kPiLog2e * L.kx * L.kx) : 0.f;
         pa.inv_wmax = 1.0f / r.weight_max;
         pa.fold = std::max(1, plan.jobs[j].fold);
+        pa.exch = plan.jobs[j].exch;
         pa.out = const_cast<unsigned char*>(plan.jobs[j].blocks);
         const int t = plan.nyq_job_of_group[g];
         pa.out_nyq = t < 0 ? nullptr : const_cast<unsigned char*>(plan.jobs[t].blocks);
