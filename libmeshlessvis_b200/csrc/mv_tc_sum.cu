@@ -14,6 +14,13 @@
 // term separately (meshless_vis/fourier_transform.cu:100-130); no reference
 // code has this factorisation.
 //
+// A CTA-pair MMA of K = 16 costs about the same whatever its N up to 256, so
+// jobs are shaped for N = 256 (128 frequency columns per n-tile): groups of
+// pure phases fold F rows of b into the columns (rows (a, bh), columns (b mod
+// F, c); TcJob::fold), and groups with per-particle Gaussian factors on
+// lattices with more b values than planes exchange the axes (rows (a, c),
+// columns b; TcJob::exch).
+//
 // Real embedding with re/im interleaved along K (k = 2j + {0,1}):
 //   A'[m, 2j..2j+1] = (Re A, Im A),  B'_re[2j..2j+1, n] = (Re B, -Im B),
 //   B'_im[2j..2j+1, n] = (Im B, Re B);  C = A' [B'_re | B'_im] = [Re F | Im F].
