@@ -1444,6 +1444,37 @@ __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, 
     const size_t rbase = (size_t)rank * J.rank_stride;
     const float* row = static_cast<const float*>(J.slots) + rbase + rl * 4;
     const double* row64 = static_cast<const double*>(J.slots) + rbase + rl * 2;
+    if (!J.slot_fp64 && nc == kReduceC && J.n_splits == 1) {
+        // the common h-bin case (one particle chunk, FP32 slots): two column
+        // blocks per round, so each thread has twice the loads in flight
+        const size_t lbase = (size_t)m_tile * J.n_ntiles;
+        for (int q = 0; q < J.blocks; q += 2) {
+            const bool two = q + 1 < J.blocks;
+            const int4 m0 = __ldg(J.colmap + (q * J.fold + bl) * J.period + c0);
+            const int4 m1 = two ? __ldg(J.colmap + ((q + 1) * J.fold + bl) * J.period + c0) : m0;
+            const float* v0 = row + (lbase + m0.x) * J.slot_stride;
+            const float* v1 = row + (lbase + m1.x) * J.slot_stride;
+            const float4 re0 = __ldg(reinterpret_cast<const float4*>(v0 + (size_t)m0.y * kM));
+            const float4 im0 = __ldg(reinterpret_cast<const float4*>(v0 + (size_t)m0.z * kM));
+            const float4 re1 = two ? __ldg(reinterpret_cast<const float4*>(v1 + (size_t)m1.y * kM)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 im1 = two ? __ldg(reinterpret_cast<const float4*>(v1 + (size_t)m1.z * kM)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            double w0[kReduceC], w1[kReduceC];
+#pragma unroll
+            for (int i = 0; i < kReduceC; ++i) {
+                w0[i] = J.coef ? (double)__ldg(J.coef + (size_t)n2[i] * J.coef_stride + q) * J.scale : J.scale;
+                w1[i] = J.coef && two ? (double)__ldg(J.coef + (size_t)n2[i] * J.coef_stride + q + 1) * J.scale
+                                      : (two ? J.scale : 0.0);
+            }
+            const float r0[kReduceC] = {re0.x, re0.y, re0.z, re0.w}, i0[kReduceC] = {im0.x, im0.y, im0.z, im0.w};
+            const float r1[kReduceC] = {re1.x, re1.y, re1.z, re1.w}, i1[kReduceC] = {im1.x, im1.y, im1.z, im1.w};
+#pragma unroll
+            for (int i = 0; i < kReduceC; ++i) {
+                sr[i] = fma(w1[i], (double)r1[i], fma(w0[i], (double)r0[i], sr[i]));
+                si[i] = fma(w1[i] * sign_im, (double)i1[i], fma(w0[i] * sign_im, (double)i0[i], si[i]));
+            }
+        }
+        return;
+    }
     for (int q = 0; q < J.blocks; ++q) {
         // column block q F + bl: Chebyshev block q (h-binned), b offset bl (folded)
         const int4 m = __ldg(J.colmap + (q * J.fold + bl) * J.period + c0);  // the same for a warp's rows
@@ -1515,42 +1546,58 @@ struct TcReduceArgs {
     bool nyquist;
 };
 
-__global__ void __launch_bounds__(256) tc_reduce_kernel(TcReduceArgs f) {
-    extern __shared__ ReduceJob s_jobs[];  // n_list (+ n_neg) descriptors
-    const int n_all = f.n_list + (f.nyquist ? f.n_neg : 0);
+// Warps per block of the reduction kernels (each sums every eighth job).
+constexpr int kReduceWarps = 8;
+
+// The Nyquist plane of one output class, with the job list split over warps
+// as in tc_reduce_planes_kernel: a block takes 32 elements (lanes), warp w
+// sums the jobs w, w + 8, ... of the element's sign of a, and the eight
+// partial sums are added in warp order (a fixed order).
+__global__ void __launch_bounds__(32 * kReduceWarps) tc_reduce_kernel(TcReduceArgs f) {
+    extern __shared__ __align__(16) unsigned char s_raw[];  // descriptors, then the partial sums
+    ReduceJob* s_jobs = reinterpret_cast<ReduceJob*>(s_raw);
+    const int n_all = f.n_list + f.n_neg;
     for (int i = threadIdx.x; i < n_all; i += blockDim.x)
         s_jobs[i] = reduce_job(f.jobs[i < f.n_list ? f.list[i] : f.list_neg[i - f.n_list]]);
+    double2* s_part = reinterpret_cast<double2*>(s_raw + (((size_t)n_all * sizeof(ReduceJob) + 15) & ~(size_t)15));
     __syncthreads();
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long rows = (long long)f.kx * f.ky;
-    const int groups = f.nyquist ? 1 : f.lz_tc / kReduceC;  // lz_tc is a multiple of 8
-    if (q >= rows * groups) return;
-    const int rho = (int)(q % rows);
+    const long long e = (long long)blockIdx.x * 32 + lane;
+    const bool active = e < rows;
+    const int rho = active ? (int)e : 0;
     const int a_idx = rho / f.ky, b_idx = rho % f.ky;
     const int a = a_idx - f.kx / 2, b = b_idx - f.ky / 2;
-    const int c0 = f.nyquist ? f.lz_tc : (int)(q / rows) * kReduceC;
-    const int nc = f.nyquist ? 1 : kReduceC;
+    const int c = f.lz_tc;
     int n2[kReduceC];
 #pragma unroll
-    for (int i = 0; i < kReduceC; ++i) n2[i] = a * a + b * b + (c0 + i) * (c0 + i);
+    for (int i = 0; i < kReduceC; ++i) n2[i] = a * a + b * b + (c + i) * (c + i);
     double sr[kReduceC] = {}, si[kReduceC] = {};
-    if (!f.nyquist) {
-        for (int j = 0; j < f.n_list; ++j) reduce_add(s_jobs[j], rho, c0, n2, nc, sr, si, 1.0);
-    } else if (a >= 0) {
-        for (int j = 0; j < f.n_list; ++j) reduce_add(s_jobs[j], b_idx, a, n2, 1, sr, si, 1.0);
-    } else {
-        for (int j = 0; j < f.n_neg; ++j)
-            reduce_add(s_jobs[f.n_list + j], f.ky - 1 - b_idx, -a - 1, n2, 1, sr, si, -1.0);
+    if (active) {
+        // for a >= 0 the a >= 0 jobs at row b_idx and column a; for a < 0 the
+        // conjugate of the a < 0 jobs at row Ky - 1 - b_idx (frequency -b) and
+        // column -a - 1 (frequency -a)
+        if (a >= 0) {
+            for (int j = warp; j < f.n_list; j += kReduceWarps) reduce_add(s_jobs[j], b_idx, a, n2, 1, sr, si, 1.0);
+        } else {
+            for (int j = warp; j < f.n_neg; j += kReduceWarps)
+                reduce_add(s_jobs[f.n_list + j], f.ky - 1 - b_idx, -a - 1, n2, 1, sr, si, -1.0);
+        }
     }
-#pragma unroll
-    for (int i = 0; i < kReduceC; ++i) {
-        if (i >= nc) break;
-        double factor = f.scale;
-        if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[i]) * f.h);
-        const size_t idx = (size_t)rho * f.lz_out + c0 + i;
-        const float2 o = f.out[idx];
-        f.out[idx] = make_float2(o.x + (float)(sr[i] * factor), o.y + (float)(si[i] * factor));
+    s_part[warp * 32 + lane] = make_double2(sr[0], si[0]);
+    __syncthreads();
+    if (warp != 0 || !active) return;
+    double tr = 0.0, ti = 0.0;
+    for (int w = 0; w < kReduceWarps; ++w) {
+        const double2 v = s_part[w * 32 + lane];
+        tr += v.x;
+        ti += v.y;
     }
+    double factor = f.scale;
+    if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[0]) * f.h);
+    const size_t idx = (size_t)rho * f.lz_out + c;
+    const float2 o = f.out[idx];
+    f.out[idx] = make_float2(o.x + (float)(tr * factor), o.y + (float)(ti * factor));
 }
 
 // The planes c < lz_tc of one output class, with the job list split over
@@ -1558,8 +1605,7 @@ __global__ void __launch_bounds__(256) tc_reduce_kernel(TcReduceArgs f) {
 // w + 8, ..., and the eight partial sums are added in warp order (a fixed
 // order: the result does not depend on timing), so eight independent load
 // chains per element hide the slots' latency.
-constexpr int kReduceWarps = 8;
-__global__ void __launch_bounds__(32 * kReduceWarps) tc_reduce_planes_kernel(TcReduceArgs f) {
+__global__ void __launch_bounds__(32 * kReduceWarps, 2) tc_reduce_planes_kernel(TcReduceArgs f) {
     extern __shared__ __align__(16) unsigned char s_raw[];  // n_list descriptors, then the partial sums
     ReduceJob* s_jobs = reinterpret_cast<ReduceJob*>(s_raw);
     for (int i = threadIdx.x; i < f.n_list; i += blockDim.x) s_jobs[i] = reduce_job(f.jobs[f.list[i]]);
@@ -2623,10 +2669,11 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             f.n_neg = (int)c.nyq_neg.size();
             f.nyquist = true;
             const long long plane = (long long)c.kx * c.ky;
-            const size_t smem = (size_t)(f.n_list + f.n_neg) * sizeof(ReduceJob);
+            const size_t smem = (((size_t)(f.n_list + f.n_neg) * sizeof(ReduceJob) + 15) & ~(size_t)15) +
+                                (size_t)32 * kReduceWarps * sizeof(double2);
             st = reduce_smem(tc_reduce_kernel, smem);
             if (st != kOk) return st;
-            tc_reduce_kernel<<<(unsigned)((plane + 255) / 256), 256, smem, stream>>>(f);
+            tc_reduce_kernel<<<(unsigned)((plane + 31) / 32), 32 * kReduceWarps, smem, stream>>>(f);
             count_launch();
         }
     }
