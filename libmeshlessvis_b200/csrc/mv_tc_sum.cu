@@ -1522,14 +1522,13 @@ __device__ __forceinline__ void reduce_add(const ReduceJob& J, int rho, int c0, 
 }
 
 // The jobs of one output class (same spectrum, same per-frequency factor)
-// -> its float2 spectrum, added: planes c in [0, lz_tc), or (nyquist) the
-// plane c = lz_tc from the transposed jobs: for a >= 0 the a >= 0 jobs at row
-// b_idx and column a; for a < 0 the conjugate of the a < 0 jobs at row
-// Ky - 1 - b_idx (frequency -b) and column -a - 1 (frequency -a).  Times the
-// factored Phi^(|k| h) in FP64 and the scale.  Thread: kReduceC consecutive
-// planes of one row (nyquist: one element), rows fastest (the slots' reads
-// are coalesced); the block gathers the class's job descriptors in shared
-// memory first.
+// -> its float2 spectrum, added: planes c in [0, lz_tc) (tc_reduce_planes_kernel),
+// or the Nyquist plane c = lz_tc from the transposed jobs (tc_reduce_kernel):
+// for a >= 0 the a >= 0 jobs at row b_idx and column a; for a < 0 the
+// conjugate of the a < 0 jobs at row Ky - 1 - b_idx (frequency -b) and column
+// -a - 1 (frequency -a).  Times the factored Phi^(|k| h) in FP64 and the
+// scale.  The kernels gather the class's job descriptors in shared memory
+// first.
 struct TcReduceArgs {
     const TcJob* jobs;
     const int* list;      // planes: the class's jobs; nyquist: its a >= 0 jobs
@@ -1543,7 +1542,6 @@ struct TcReduceArgs {
     bool factored;
     double scale;
     float2* out;
-    bool nyquist;
 };
 
 // Warps per block of the reduction kernels (each sums every eighth job).
@@ -2652,7 +2650,6 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         f.factored = c.factored;
         f.scale = c.scale;
         f.out = c.out;
-        f.nyquist = false;
         if (f.n_list > 0) {
             const long long blocks = ((long long)c.kx * c.ky + 31) / 32 * (c.lz_tc / kReduceC);
             const size_t smem = (((size_t)f.n_list * sizeof(ReduceJob) + 15) & ~(size_t)15) +
@@ -2667,7 +2664,6 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             f.n_list = (int)c.nyq_pos.size();
             f.list_neg = lists + c.jobs.size() + c.nyq_pos.size();
             f.n_neg = (int)c.nyq_neg.size();
-            f.nyquist = true;
             const long long plane = (long long)c.kx * c.ky;
             const size_t smem = (((size_t)(f.n_list + f.n_neg) * sizeof(ReduceJob) + 15) & ~(size_t)15) +
                                 (size_t)32 * kReduceWarps * sizeof(double2);
