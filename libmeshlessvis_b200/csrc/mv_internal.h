@@ -298,7 +298,7 @@ struct TensorPlan {
     std::vector<TcJob> jobs;
     std::vector<int2> items;  // 128x128-tile items (n_narrow), narrow CTA-pair items (n_pair_narrow),
                               // CTA-pair items (n_pair), then 128x256
-    int n_narrow = 0, n_pair_narrow = 0, n_pair = 0;
+    int n_narrow = 0, n_pair_narrow = 0, n_pair = 0, n_pair_db = 0;
     std::vector<Class> classes;
     std::vector<int> group_class, job_of_group;
     std::vector<int> nyq_job_of_group;  // the transposed Nyquist-plane jobs (a >= 0 here, a < 0 next), or -1

@@ -160,9 +160,16 @@ constexpr unsigned long long kAbortGraceNs = 200000ull;
 //       alternating 128-column accumulators per CTA as in kNarrow.  Each CTA
 //       reads A and half of B, 96 B/clk at the tensor core's rate, where a
 //       128x128 MMA needs the port's full 128 B/clk; B work per CTA halves.
-enum TileMode : int { kNarrow = 0, kWide = 1, kPair = 2, kPairNarrow = 3 };
+//   kPairDB: kPair for jobs of short items (at most kDBMaxChains chains): two
+//       alternating 256-column accumulators fill all of TMEM, so the MMAs go
+//       on while a flush reads the finished one, and the flush adds it into
+//       the item's FP32 slot directly (a read-modify-write in L2; the item's
+//       few chains keep its slot there).  Long items keep kPair, whose
+//       per-chain slot traffic would no longer stay in L2.
+enum TileMode : int { kNarrow = 0, kWide = 1, kPair = 2, kPairNarrow = 3, kPairDB = 4 };
+constexpr int kDBMaxChains = 8;
 
-constexpr bool pair_mode(int mode) { return mode == kPair || mode == kPairNarrow; }
+constexpr bool pair_mode(int mode) { return mode == kPair || mode == kPairNarrow || mode == kPairDB; }
 constexpr bool narrow_mode(int mode) { return mode == kNarrow || mode == kPairNarrow; }
 
 template <int MODE>
@@ -181,7 +188,8 @@ struct Shape {
     static constexpr int kBStages = MODE == kWide ? 2 : 4;
     static constexpr int kSlots = 2;
     static constexpr int kFull = kAStages > kBStages ? kAStages : kBStages;
-    static constexpr int kBufs = narrow_mode(MODE) ? 2 : 1;  // TMEM accumulators, kN columns each
+    static constexpr bool kDB = MODE == kPairDB;              // totals in the slot, no TMEM total
+    static constexpr int kBufs = narrow_mode(MODE) || kDB ? 2 : 1;  // TMEM accumulators, kN columns each
     static constexpr int kBBytes = kBRows * kRowBytes;
     static constexpr int kAStageBytes = 2 * kABytes;  // A_hi, A_lo
     static constexpr int kBStageBytes = 2 * kBBytes;  // B_hi, B_lo (2 bnc rows each, packed)
@@ -808,6 +816,36 @@ __global__ void __launch_bounds__(kThreads, 1) tc_sum_kernel(TcArgs a) {
                 // warp-uniform outcome: the warp arrives as one below
                 if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], u & 1, abort_flag, a.error_flag, a.wait_limit_ns, 4))) break;
                 tc_fence_after();
+                if constexpr (SH::kDB) {
+                    // the item's FP32 total is its slot: the first chain stores
+                    // it, later ones add to it (the slot's loads are issued
+                    // before the TMEM reads so their latency overlaps them);
+                    // 16 columns per round trip
+#pragma unroll 1
+                    for (int cc = 0; cc < ncols; cc += 16) {
+                        float4 sv[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            sv[i] = kk == 0 ? make_float4(0.f, 0.f, 0.f, 0.f)
+                                            : __ldcg(reinterpret_cast<const float4*>(slot32 + (size_t)(cc + 4 * i) * kM));
+                        float dv[16];
+                        tmem_ld8(acc_col + cc, dv);
+                        tmem_ld8(acc_col + cc + 8, dv + 8);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            __stcg(reinterpret_cast<float4*>(slot32 + (size_t)(cc + 4 * i) * kM),
+                                   make_float4(sv[i].x + dv[4 * i], sv[i].y + dv[4 * i + 1], sv[i].z + dv[4 * i + 2],
+                                               sv[i].w + dv[4 * i + 3]));
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (rank == 0) mbar_arrive(&acc_empty[b]);
+                        else mbar_arrive_leader(&acc_empty[b]);
+                    }
+                    continue;
+                }
                 tmem_wait_st();  // the previous flush's stores of the total
                 // the chain partials are summed into an FP32 total in TMEM, over
                 // at most kMaxItemChains chains; then (and at the item's end)
@@ -1653,6 +1691,15 @@ bool is_spectrum_lattice(const Lattice& L) {
            L.m[6] == 0 && L.m[7] == 0;
 }
 
+// kPairDB tiles: MV_TC_DB=0 turns them off (those jobs then take kPair).
+bool tc_db_enabled() {
+    static const bool v = [] {
+        const char* e = std::getenv("MV_TC_DB");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
 // Row folds of pure-phase groups: MV_TC_FOLD=0 turns them off.
 bool tc_fold_enabled() {
     static const bool v = [] {
@@ -2007,6 +2054,9 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         const long long chunk = ((j.n + splits - 1) / splits + kKp - 1) / kKp * kKp;
         splits = (j.n + chunk - 1) / chunk;
         j.slot_fp64 = chunk > max_chunk ? 1 : 0;
+        // short items of a CTA-pair job: double-buffered accumulators
+        if (mode == kPair && (chunk / kKp + flush_stages - 1) / flush_stages <= kDBMaxChains && tc_db_enabled())
+            mode = kPairDB;
         j.k_chunk = (int)chunk;
         j.n_splits = (int)splits;
         j.ctas = ctas;
@@ -2264,7 +2314,7 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
     // split) over distinct m-tiles, all of them reading the same B-operand
     // stages (images) at about the same time, and the next waves the other
     // jobs' items of the same m-tiles.
-    auto order = [](int m) { return m == kNarrow ? 0 : m == kPairNarrow ? 1 : m == kPair ? 2 : 3; };
+    auto order = [](int m) { return m == kNarrow ? 0 : m == kPairNarrow ? 1 : m == kPair ? 2 : m == kPairDB ? 3 : 4; };
     const int sms = std::max(2, device_sm_count());
     for (Item& it : items) {
         it.cost_class = (int)std::floor(std::log((double)std::max(1LL, it.cost)) / std::log(1.05));
@@ -2279,12 +2329,13 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
         return x.item.y < y.item.y;
     });
     plan.items.reserve(items.size());
-    plan.n_narrow = plan.n_pair_narrow = plan.n_pair = 0;
+    plan.n_narrow = plan.n_pair_narrow = plan.n_pair = plan.n_pair_db = 0;
     for (auto& it : items) {
         plan.items.push_back(it.item);
         plan.n_narrow += it.mode == kNarrow ? 1 : 0;
         plan.n_pair_narrow += it.mode == kPairNarrow ? 1 : 0;
         plan.n_pair += it.mode == kPair ? 1 : 0;
+        plan.n_pair_db += it.mode == kPairDB ? 1 : 0;
     }
     const size_t jobs_bytes = ((plan.jobs.size() * sizeof(TcJob) + 255) / 256) * 256;
     plan.meta_bytes = jobs_bytes + ((plan.items.size() * sizeof(int2) + 255) / 256) * 256;
@@ -2595,12 +2646,13 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
     // one persistent launch per tile mode for all groups
     if (!plan.items.empty()) {
         timer_begin(timer, 3, stream);
-        const int counts[4] = {plan.n_narrow, plan.n_pair_narrow, plan.n_pair,
-                               (int)plan.items.size() - plan.n_narrow - plan.n_pair_narrow - plan.n_pair};
-        const int modes[4] = {kNarrow, kPairNarrow, kPair, kWide};
+        const int counts[5] = {plan.n_narrow, plan.n_pair_narrow, plan.n_pair, plan.n_pair_db,
+                               (int)plan.items.size() - plan.n_narrow - plan.n_pair_narrow - plan.n_pair -
+                                   plan.n_pair_db};
+        const int modes[5] = {kNarrow, kPairNarrow, kPair, kPairDB, kWide};
         int first = 0;
         bool hooked = false;
-        for (int m = 0; m < 4 && st == kOk; first += counts[m], ++m) {
+        for (int m = 0; m < 5 && st == kOk; first += counts[m], ++m) {
             TcArgs a;
             a.jobs = static_cast<const TcJob*>(plan.d_jobs);
             a.items = static_cast<const int2*>(plan.d_items) + first;
@@ -2622,6 +2674,7 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             case kNarrow: st = launch_tile<kNarrow>(a, stream); break;
             case kPairNarrow: st = launch_tile<kPairNarrow>(a, stream); break;
             case kPair: st = launch_tile<kPair>(a, stream); break;
+            case kPairDB: st = launch_tile<kPairDB>(a, stream); break;
             default: st = launch_tile<kWide>(a, stream); break;
             }
             if (st != kOk) break;
