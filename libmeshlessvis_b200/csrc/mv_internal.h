@@ -270,14 +270,15 @@ struct TensorPlan {
         int group;
         int nbins;
         size_t meta_offset;     // edges, then int4 bin table, then float2 bin scales
-        size_t cursor_offset;   // into acc (ints)
         size_t coef_offset;     // into coef (floats)
         size_t coef_count;
         int nsq;                // |k|^2 / step^2 values: max a^2 + b^2 + c^2 + 1
         int total_q;            // Chebyshev blocks over all bins: the table's stride per |k|^2
         std::vector<HBin> bins;
         std::vector<float> edges;  // nbins + 1: the fine edges where the bins start (classification)
-        size_t sorted_offset;      // into TensorWorkspace::sorted: n float4, then n radii (256-aligned)
+        size_t sorted_offset;      // into TensorWorkspace::sorted: n float4, n radii, then the radius sort's
+                                   // keys and indices (in, out) and temporary storage (256-aligned)
+        size_t sort_temp_bytes;
     };
     size_t sorted_bytes = 0;
     std::vector<Binned> binned;
@@ -318,7 +319,7 @@ struct TensorPlan {
     std::vector<size_t> tp_offset, tp_nyq_offset;
     std::vector<size_t> bimg_offset;  // per job: its B-operand images in the workspace, or SIZE_MAX
     size_t bimg_bytes = 0;
-    size_t tp_bytes = 0, acc_bytes = 0, meta_bytes = 0;
+    size_t tp_bytes = 0, meta_bytes = 0;
     const void* d_jobs = nullptr;
     const void* d_items = nullptr;
     int flush = 16;        // stages per TMEM accumulation chain of the kWide / kPair tiles, as planned
@@ -327,7 +328,6 @@ struct TensorPlan {
 
 struct TensorWorkspace {
     Workspace particles;  // per-particle constants of every group
-    Workspace acc;        // per-compute counters (zeroed each compute)
     Workspace slots;      // work items' totals (FP32 or FP64)
     Workspace meta;       // job and item tables
     Workspace bimg;       // B-operand images
@@ -344,7 +344,6 @@ struct TensorWorkspace {
         plan_key.clear();
         plan.reset();
         particles.release();
-        acc.release();
         slots.release();
         meta.release();
         bimg.release();

@@ -266,6 +266,7 @@ struct FoldKernelArgs {
     float shell_r0;
     const uint32_t* shell_reps;  // representatives sorted by |k|: x | y << 10 | z << 20
     int shell_count;
+    const float* shell_radii;    // the particles' radii, ascending within each bin
 };
 
 template <int L, int FY, int AMP>
@@ -332,21 +333,35 @@ __global__ void __launch_bounds__(kThreads, 2) fold_sum_kernel(FoldKernelArgs fa
     int rb[kShell ? L : 1];
     int beg = blockIdx.y * a.chunk, end = min(a.n, beg + a.chunk), w_lo = 0, w_hi = a.n;
     if constexpr (kShell) {
-        int bmin = fa.shell_nbins, bmax = -1;
+        int bmin = fa.shell_nbins, bmax = -1, cut = 0;
 #pragma unroll
         for (int m = 0; m < L; ++m) {
-            rb[m] = hbin_of(fa.shell_edges, fa.shell_nbins, r[m] > 0.f ? fa.shell_r0 / r[m] : INFINITY);
+            const float hstar = r[m] > 0.f ? fa.shell_r0 / r[m] : INFINITY;
+            rb[m] = hbin_of(fa.shell_edges, fa.shell_nbins, hstar);
             bmin = min(bmin, rb[m]);
             bmax = max(bmax, rb[m]);
+            // the bin's particles are sorted by radius, and Phi^ - C is zero
+            // from the branch point on (h |k| >= r0): only the run below
+            // h* = r0 / |k| counts (with a margin of 1e-5 of h* for rounding)
+            int lo = fa.shell_first[rb[m]], hi = fa.shell_first[rb[m] + 1];
+            const float hcut = hstar * 1.00001f;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (fa.shell_radii[mid] < hcut) lo = mid + 1;
+                else hi = mid;
+            }
+            cut = max(cut, lo);
         }
         if (!active) {
             bmin = fa.shell_nbins;
             bmax = -1;
+            cut = 0;
         }
         bmin = __reduce_min_sync(0xffffffffu, bmin);
         bmax = __reduce_max_sync(0xffffffffu, bmax);
+        cut = __reduce_max_sync(0xffffffffu, cut);
         w_lo = bmax < 0 ? 0 : fa.shell_first[bmin];
-        w_hi = bmax < 0 ? 0 : fa.shell_first[bmax + 1];
+        w_hi = bmax < 0 ? 0 : cut;
         __shared__ int s_lo, s_hi;
         if (tid == 0) {
             s_lo = a.n;
@@ -809,6 +824,7 @@ int launch_plain_sum(const SumRequest& req, Workspace& ws, KernelTimer* timer) {
         fa.shell_first = req.shell_first;
         fa.shell_r0 = (float)phi_branch_point(req.basis);
         fa.shell_reps = shell_reps;
+        fa.shell_radii = req.kink ? req.radii : nullptr;
         fa.shell_count = (int)threads;
         FoldKernel k = amp == kAmpShell ? fold_sum_kernel<1, 2, kAmpShell>
                        : !fold_y      ? pick_fold<8, 1>(amp)

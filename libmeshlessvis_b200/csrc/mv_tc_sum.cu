@@ -93,6 +93,8 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "meshless_vis_b200.h"
 #include "mv_device.cuh"
 #include "mv_internal.h"
@@ -1240,7 +1242,6 @@ struct TcBinnedPrepArgs {
     const float* edges;    // nbins + 1 classification edges
     const int4* bins;      // (first block, capacity, coef offset, order)
     const float4* spans;   // (lo, hi, 2^12 / W_b, 0): Chebyshev interval and weight scale
-    int* cursors;          // nbins, zero at launch
     uint8_t* out;          // the group's blocks, bin by bin
     uint8_t* out_nyq;      // the same with x and z exchanged, or null
     const int* first;      // nbins + 1: the bins' first particles in sorted order
@@ -1248,19 +1249,32 @@ struct TcBinnedPrepArgs {
     float* sorted_radii;
     int* error_flag;
     int fold;              // the bins' planes jobs' row fold (1: none): their y rotation covers fold steps
+    const int* order;      // the particles by ascending radius (bins are runs of it)
 };
 
-// Scatters each particle's constants into its bin's blocks (order within a
-// bin follows the atomic counter); gam holds t, the normalised radius.  The
-// blocks were zeroed first, so padding particles have zero amplitude.
-__global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
+// Sort keys of a binned group: radii (non-negative, so their bits order as
+// the values) and the particles' indices.
+__global__ void tc_radius_keys_kernel(const float* radii, int n, uint32_t* keys, int* index) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= p.n) return;
+    if (j >= n) return;
+    keys[j] = __float_as_uint(radii[j]);
+    index[j] = j;
+}
+
+// Writes each particle's constants into its bin's blocks, in ascending radius
+// (`order`, from a stable radix sort: the same order on every compute, and
+// the branch part can stop at the first radius past r0 / |k|); gam holds t,
+// the normalised radius.  The blocks were zeroed first, so padding particles
+// have zero amplitude.
+__global__ void tc_prep_binned_kernel(TcBinnedPrepArgs p) {
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;  // in the radius order
+    if (pos >= p.n) return;
+    const int j = p.order[pos];
     const float h = p.radii[j];
     const int b = hbin_of(p.edges, p.nbins, h);
     const int4 bin = p.bins[b];
-    const int slot = atomicAdd(p.cursors + b, 1);
-    if (slot >= bin.y) {  // the registered histogram does not hold for these radii
+    const int slot = pos - p.first[b];
+    if (slot < 0 || slot >= bin.y) {  // the registered histogram does not hold for these radii
         atomicOr(p.error_flag, 2048);
         return;
     }
@@ -2159,10 +2173,20 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
             bg.edges.push_back(r.hbins->edges[kHBinFine]);
             bg.nsq = (int)(lattice_nsq(L) + 1);
             bg.meta_offset = 0;  // placed by tensor_reserve_upload
-            bg.cursor_offset = plan.acc_bytes;
-            plan.acc_bytes += ((size_t)bg.nbins * sizeof(int) + 255) / 256 * 256;
             bg.sorted_offset = plan.sorted_bytes;
-            plan.sorted_bytes += ((size_t)r.n * sizeof(float4) + 255) / 256 * 256 + ((size_t)r.n * sizeof(float) + 255) / 256 * 256;
+            {
+                // sorted particles, their radii, then the radix sort's keys,
+                // indices (in and out) and temporary storage
+                size_t temp = 0;
+                const int sst = check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, temp, (const uint32_t*)nullptr,
+                                                                           (uint32_t*)nullptr, (const int*)nullptr,
+                                                                           (int*)nullptr, r.n),
+                                           "radius sort size");
+                if (sst != kOk) return sst;
+                bg.sort_temp_bytes = temp;
+                const size_t a4 = ((size_t)r.n * 4 + 255) / 256 * 256;
+                plan.sorted_bytes += ((size_t)r.n * sizeof(float4) + 255) / 256 * 256 + 5 * a4 + (temp + 255) / 256 * 256;
+            }
             bg.coef_offset = plan.coef_bytes / sizeof(float);
             std::vector<int> first_block(bg.nbins);
             long long blocks = 0;
@@ -2373,7 +2397,6 @@ int tensor_plan(const std::vector<SumRequest>& groups, TensorPlan& plan) {
 
 int tensor_reserve_upload(TensorPlan& plan, TensorWorkspace& ws, cudaStream_t stream) {
     int st = ws.particles.reserve(std::max<size_t>(plan.tp_bytes, 256));
-    if (st == kOk) st = ws.acc.reserve(std::max<size_t>(plan.acc_bytes, 256));
     if (st == kOk) st = ws.meta.reserve(std::max<size_t>(plan.meta_bytes, 256));
     if (st == kOk && plan.bimg_bytes) st = ws.bimg.reserve(plan.bimg_bytes);
     if (st == kOk && plan.coef_bytes) st = ws.coef.reserve(plan.coef_bytes);
@@ -2549,10 +2572,6 @@ int reduce_smem(void (*kernel)(TcReduceArgs), size_t bytes) {
 int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan, TensorWorkspace& ws,
                    Workspace& plain_ws, KernelTimer* timer, cudaStream_t stream, int* error_flag) {
     int st = kOk;
-    // zero the per-compute counters (h-bin scatter cursors)
-    if (plan.acc_bytes)
-        st = check_cuda(cudaMemsetAsync(ws.acc.ptr, 0, plan.acc_bytes, stream), "cudaMemsetAsync(acc)");
-    if (st != kOk) return st;
     // per-particle constants of every group
     for (size_t g = 0; g < groups.size(); ++g) {
         const int j = plan.job_of_group[g];
@@ -2582,7 +2601,6 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             bp.edges = reinterpret_cast<const float*>(meta);
             bp.bins = reinterpret_cast<const int4*>(meta + edges_bytes);
             bp.spans = reinterpret_cast<const float4*>(bp.bins + bg.nbins);
-            bp.cursors = reinterpret_cast<int*>(static_cast<char*>(ws.acc.ptr) + bg.cursor_offset);
             bp.out = reinterpret_cast<uint8_t*>(tp);
             bp.out_nyq = reinterpret_cast<uint8_t*>(tpn);
             bp.first = reinterpret_cast<const int*>(bp.spans + bg.nbins);
@@ -2591,6 +2609,26 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
             bp.sorted_radii = reinterpret_cast<float*>(sorted + ((size_t)r.n * sizeof(float4) + 255) / 256 * 256);
             bp.error_flag = error_flag;
             bp.fold = std::max(1, plan.jobs[j].fold);
+            {
+                // the particles in ascending radius (stable: ties keep their
+                // index order), so every bin is a run of it, in the same order
+                // on every compute
+                const size_t a4 = ((size_t)r.n * 4 + 255) / 256 * 256;
+                char* base = sorted + ((size_t)r.n * sizeof(float4) + 255) / 256 * 256 + a4;
+                uint32_t* keys_in = reinterpret_cast<uint32_t*>(base);
+                uint32_t* keys_out = reinterpret_cast<uint32_t*>(base + a4);
+                int* index_in = reinterpret_cast<int*>(base + 2 * a4);
+                int* index_out = reinterpret_cast<int*>(base + 3 * a4);
+                void* temp = base + 4 * a4;
+                size_t temp_bytes = bg.sort_temp_bytes;
+                tc_radius_keys_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(r.radii, r.n, keys_in, index_in);
+                count_launch();
+                st = check_cuda(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, index_in, index_out,
+                                                                r.n, 0, 32, stream),
+                                "radius sort");
+                if (st != kOk) return st;
+                bp.order = index_out;
+            }
             tc_prep_binned_kernel<<<(r.n + 255) / 256, 256, 0, stream>>>(bp);
             count_launch();
             TcCoefArgs ca;
