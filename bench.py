@@ -470,8 +470,11 @@ def run_ours(args):
         best_ms = sp.autotune(cfg, ds, form)
         vals = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
         lib.vis_autotune_lookup(M.int3(*w["grid"]), n, len(w["groups"]), form, *[ctypes.byref(x) for x in vals])
+        shapes = [ctypes.c_int(), ctypes.c_int()]
+        lib.vis_autotune_lookup_shapes(M.int3(*w["grid"]), n, len(w["groups"]), form,
+                                       *[ctypes.byref(x) for x in shapes])
         tuned = {"plain_waves": vals[0].value, "tensor_waves": vals[1].value, "tensor_flush_stages": vals[2].value,
-                 "best_sum_ms": best_ms}
+                 "tile_shapes": shapes[0].value, "hbin_price": shapes[1].value, "best_sum_ms": best_ms}
     for _ in range(max(3, args.warmup)):
         step()
     cfg.synchronize()

@@ -100,20 +100,44 @@ int vis_spectrum_render_views(VisSpectrum* spectrum, VisConfig* vis_config, int 
 /* Picks the launch parameters of vis_spectrum_compute for this spectrum's
  * shape (lattice, total particles of the dataset, number of groups, form) by
  * timing candidates on the caller's data: the plain form's split-K (2, 4, 6, 8
- * blocks per SM), the tensor form's particle splits (2, 4, 8 waves) and the
+ * blocks per SM), the tensor form's particle splits (2, 4, 8 waves), the
  * accumulation chain of its single-accumulator tiles (8 or 16 stages; longer
- * chains lose accuracy; the double-buffered tile keeps at most 8).  Each
- * candidate runs vis_spectrum_compute twice (the spectrum holds the last
- * result); the best set is kept for the process and used by later computes of
- * the same shape.  best_ms (may be NULL) receives its time.  No counterpart in
- * the reference, which fixes its launch shape by block_length and
- * number_of_partial_sums. */
+ * chains lose accuracy; the double-buffered tile keeps at most 8), its tile
+ * shapes (each VIS_TILE_* shape turned off in turn, for the tensor and auto
+ * forms) and, for datasets with h-binned groups, the price of one more h-bin
+ * (256, 1024, 4096: the h-bin count).  Each candidate runs
+ * vis_spectrum_compute twice (the spectrum holds the last result); the best
+ * set is kept for the process and used by later computes of the same shape.
+ * best_ms (may be NULL) receives its time.  No counterpart in the reference,
+ * which fixes its launch shape by block_length and number_of_partial_sums
+ * (fourier_transform.cu:167-180). */
 int vis_autotune_spectrum(VisSpectrum* spectrum, VisConfig* vis_config, MeshlessDataset* meshless_dataset, int form,
                           float* best_ms);
 /* The parameters that computes of this shape use; returns 1 if they were
  * tuned, 0 for the defaults (6, 4, 16). */
 int vis_autotune_lookup(int3 grid_size, long long number_of_terms, int number_of_groups, int form,
                         int* plain_waves, int* tensor_waves, int* tensor_flush_stages);
+/* Tile shapes of the tensor form, as bits: the planner uses a shape where its
+ * cost rule finds it cheaper, and only if its bit is set. */
+enum {
+    VIS_TILE_ROW_FOLD = 1,       /* several b rows of a job as column blocks of one row */
+    VIS_TILE_AXIS_EXCHANGE = 2,  /* rows (a, c) and columns b for Gaussian jobs */
+    VIS_TILE_DOUBLE_BUFFER = 4,  /* two accumulators per CTA pair for jobs of short items */
+    VIS_TILE_CTA_PAIRS = 8,      /* CTA-pair (M = 256) tiles at all */
+    VIS_TILE_ALL = 15
+};
+/* The tile shapes (VIS_TILE_* bits) and the h-bin price that computes of this
+ * shape use; returns 1 if they were tuned, 0 for the defaults (VIS_TILE_ALL,
+ * 1024).  Either pointer may be NULL. */
+int vis_autotune_lookup_shapes(int3 grid_size, long long number_of_terms, int number_of_groups, int form,
+                               int* tile_shapes, int* hbin_price);
+/* Records a parameter set for a shape, as a tuning run would: for example one
+ * read back by the two lookups in an earlier process, or tile shapes a caller
+ * wants kept off.  Every value must lie in its candidate set above
+ * (tile_shapes 0 .. VIS_TILE_ALL, hbin_price 1 .. 2^20); else
+ * VIS_ERROR_INVALID_VALUE and nothing is recorded. */
+int vis_autotune_store(int3 grid_size, long long number_of_terms, int number_of_groups, int form, int plain_waves,
+                       int tensor_waves, int tensor_flush_stages, int tile_shapes, int hbin_price);
 void vis_autotune_clear(void);
 
 /* Device memory the tensor form may use for B-operand images (the c-axis

@@ -37,6 +37,8 @@ BASIS_NAMES = {"sph": SPH, "gaussian": GAUSSIAN, "wendland_d3_c2": WENDLAND_D3_C
 
 # include/meshless_vis_b200.h: enum VisSumForm / VisTimingStage / VisError
 FORM_AUTO, FORM_PLAIN, FORM_TENSOR = 0, 1, 2
+# include/meshless_vis_b200.h: VIS_TILE_* (tensor-form tile shapes, bits)
+TILE_ROW_FOLD, TILE_AXIS_EXCHANGE, TILE_DOUBLE_BUFFER, TILE_CTA_PAIRS, TILE_ALL = 1, 2, 4, 8, 15
 STAGE_SUM, STAGE_SLICE, STAGE_FFT, STAGE_TENSOR_SUM = 0, 1, 2, 3
 VIS_SUCCESS = 0
 
@@ -109,6 +111,8 @@ SIGNATURES = {
     "vis_spectrum_compute": (c_int, [c_void_p, PConfig, PDataset, c_int]),
     "vis_autotune_spectrum": (c_int, [c_void_p, PConfig, PDataset, c_int, POINTER(c_float)]),
     "vis_autotune_lookup": (c_int, [int3, c_longlong, c_int, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+    "vis_autotune_lookup_shapes": (c_int, [int3, c_longlong, c_int, c_int, POINTER(c_int), POINTER(c_int)]),
+    "vis_autotune_store": (c_int, [int3, c_longlong, c_int, c_int, c_int, c_int, c_int, c_int, c_int]),
     "vis_autotune_clear": (None, []),
     "vis_set_operand_cache_limit": (None, [ctypes.c_longlong]),
     "vis_tensor_wait_test_hook": (c_int, [ctypes.c_longlong]),

@@ -373,6 +373,16 @@ void timer_end(KernelTimer* timer, int stage, cudaStream_t stream);
 
 int device_sm_count();
 
+// Tile shapes of the tensor form the planner may use; mirrors the VIS_TILE_*
+// bits of meshless_vis_b200.h.
+enum TileShape : int {
+    kTileRowFold = 1,
+    kTileAxisExchange = 2,
+    kTileDoubleBuffer = 4,
+    kTileCtaPairs = 8,
+    kTileAll = 15,
+};
+
 // Launch parameters chosen per workload shape by the autotuner
 // (vis_autotune_spectrum, mv_tune.cu); defaults otherwise.  Only parameters
 // that leave results within tolerance are tuned.
@@ -383,6 +393,7 @@ struct TuneParams {
                           // the double-buffered 128x128 tile uses at most 8)
     int hbin_job_cost = 1024;  // h-binned groups: cost of one more bin (a job), in particle x n-tile units
     int hbin_block_cost = 0;  // h-binned groups: cost of one more Chebyshev block (the reduction), same units
+    int tc_shapes = kTileAll;  // tensor form: the tile shapes the planner may use (TileShape bits)
 };
 // The parameters in force on this thread: set by TuneScope around a compute.
 const TuneParams& active_tune();

@@ -1705,40 +1705,44 @@ bool is_spectrum_lattice(const Lattice& L) {
            L.m[6] == 0 && L.m[7] == 0;
 }
 
-// kPairDB tiles: MV_TC_DB=0 turns them off (those jobs then take kPair).
+// kPairDB tiles: MV_TC_DB=0 or a tuned set without kTileDoubleBuffer turns
+// them off (those jobs then take kPair).
 bool tc_db_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("MV_TC_DB");
         return !(e && e[0] == '0');
     }();
-    return v;
+    return v && (active_tune().tc_shapes & kTileDoubleBuffer);
 }
 
-// Row folds of pure-phase groups: MV_TC_FOLD=0 turns them off.
+// Row folds of pure-phase and h-binned groups: MV_TC_FOLD=0 or a tuned set
+// without kTileRowFold turns them off.
 bool tc_fold_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("MV_TC_FOLD");
         return !(e && e[0] == '0');
     }();
-    return v;
+    return v && (active_tune().tc_shapes & kTileRowFold);
 }
 
-// Axis exchange of non-folding groups: MV_TC_EXCHANGE=0 turns it off.
+// Axis exchange of non-folding groups: MV_TC_EXCHANGE=0 or a tuned set
+// without kTileAxisExchange turns it off.
 bool tc_exchange_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("MV_TC_EXCHANGE");
         return !(e && e[0] == '0');
     }();
-    return v;
+    return v && (active_tune().tc_shapes & kTileAxisExchange);
 }
 
-// kPair tiles: MV_TC_PAIRS=0 turns them off (jobs then take kWide tiles).
+// kPair tiles: MV_TC_PAIRS=0 or a tuned set without kTileCtaPairs turns them
+// off (jobs then take kWide tiles).
 bool tc_pairs_enabled() {
     static const bool v = [] {
         const char* e = std::getenv("MV_TC_PAIRS");
         return !(e && e[0] == '0');
     }();
-    return v;
+    return v && (active_tune().tc_shapes & kTileCtaPairs);
 }
 
 // Stages per TMEM accumulation chain before a flush into the FP32 total.
@@ -2476,7 +2480,7 @@ int tensor_prepare(const std::vector<SumRequest>& groups, TensorWorkspace& ws, c
     cudaGetDevice(&dev);
     put(&dev, sizeof dev);
     const TuneParams& tp = active_tune();
-    const int tune[5] = {tp.plain_waves, tp.tc_waves, tp.tc_flush, tp.hbin_job_cost, tp.hbin_block_cost};
+    const int tune[6] = {tp.plain_waves, tp.tc_waves, tp.tc_flush, tp.hbin_job_cost, tp.hbin_block_cost, tp.tc_shapes};
     put(tune, sizeof tune);
     const size_t limit = operand_cache_limit();
     put(&limit, sizeof limit);

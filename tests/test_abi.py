@@ -183,6 +183,32 @@ def test_autotune_table_starts_with_the_defaults():
     tuned = lib.vis_autotune_lookup(L.int3(64, 64, 64), 4096, 2, 0, *[ctypes.byref(v) for v in vals])
     assert tuned == 0
     assert [v.value for v in vals] == [6, 4, 16]
+    shapes = [ctypes.c_int(), ctypes.c_int()]
+    assert lib.vis_autotune_lookup_shapes(L.int3(64, 64, 64), 4096, 2, 0, *[ctypes.byref(v) for v in shapes]) == 0
+    assert [v.value for v in shapes] == [L.TILE_ALL, 1024]
+
+
+def test_autotune_store_records_a_set_and_refuses_values_outside_the_candidates():
+    """vis_autotune_store puts a parameter set in the table (host only, no
+    GPU): both lookups return it; a value outside its candidate set is refused
+    with VIS_ERROR_INVALID_VALUE and leaves the entry as it was."""
+    lib = L.load()
+    lib.vis_autotune_clear()
+    shape = (L.int3(96, 64, 32), 12345, 3, 2)
+    shapes_off = L.TILE_ALL & ~L.TILE_AXIS_EXCHANGE
+    assert lib.vis_autotune_store(*shape, 4, 8, 8, shapes_off, 256) == 0
+    vals = [ctypes.c_int() for _ in range(5)]
+    assert lib.vis_autotune_lookup(*shape, *[ctypes.byref(v) for v in vals[:3]]) == 1
+    assert lib.vis_autotune_lookup_shapes(*shape, *[ctypes.byref(v) for v in vals[3:]]) == 1
+    assert [v.value for v in vals] == [4, 8, 8, shapes_off, 256]
+    for bad in [(3, 8, 8, 0, 256), (4, 16, 8, 0, 256), (4, 8, 32, 0, 256), (4, 8, 8, 16, 256), (4, 8, 8, -1, 256),
+                (4, 8, 8, 0, 0)]:
+        assert lib.vis_autotune_store(*shape, *bad) == 1
+    assert lib.vis_autotune_store(shape[0], 12345, 3, 7, 4, 8, 8, 0, 256) == 1  # unknown form
+    assert lib.vis_autotune_lookup_shapes(*shape, *[ctypes.byref(v) for v in vals[3:]]) == 1
+    assert [v.value for v in vals[3:]] == [shapes_off, 256]
+    lib.vis_autotune_clear()
+    assert lib.vis_autotune_lookup_shapes(*shape, None, None) == 0
 
 
 def test_operand_cache_limit_setter_takes_every_form():
