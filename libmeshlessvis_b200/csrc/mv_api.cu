@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
@@ -166,19 +167,79 @@ int registration_pool(cudaMemPool_t* pool) {
     return kOk;
 }
 
+}  // namespace
+
+// Device blocks of unregistered particle arrays, kept per config for the next
+// registration of the same byte size, first in first out: a register /
+// unregister cycle per frame of the same datasets in the same order then gets
+// back the same device addresses, so a batch of them replays its CUDA graph
+// instead of running, capturing and instantiating it again (which the pool's
+// own reuse order did not guarantee).  The blocks held plus those registered
+// never exceed the most this config had registered at once; the rest go back
+// to the pool, and vis_config_destroy returns them all.
+struct RegistrationCache {
+    std::map<size_t, std::deque<void*>> blocks;
+    size_t held = 0, live = 0, peak = 0;
+
+    void* take(size_t bytes) {
+        auto it = blocks.find(bytes);
+        if (it == blocks.end()) return nullptr;
+        void* p = it->second.front();
+        it->second.pop_front();
+        if (it->second.empty()) blocks.erase(it);
+        held -= bytes;
+        return p;
+    }
+    // returns held blocks to the pool, largest first, until held + live <= peak
+    void trim(cudaStream_t stream) {
+        while (held > 0 && held + live > peak) {
+            auto it = std::prev(blocks.end());
+            cudaFreeAsync(it->second.front(), stream);
+            held -= it->first;
+            it->second.pop_front();
+            if (it->second.empty()) blocks.erase(it);
+        }
+    }
+    void registered(size_t bytes, cudaStream_t stream) {
+        live += bytes;
+        peak = std::max(peak, live);
+        trim(stream);
+    }
+    void unregistered(void* p, size_t bytes, cudaStream_t stream) {
+        live = live >= bytes ? live - bytes : 0;
+        blocks[bytes].push_back(p);
+        held += bytes;
+        trim(stream);
+    }
+    void release(cudaStream_t stream) {
+        for (auto& kv : blocks)
+            for (void* p : kv.second) cudaFreeAsync(p, stream);
+        blocks.clear();
+        held = live = peak = 0;
+    }
+};
+
+namespace {
 template <typename T>
-int registration_alloc(T** p, size_t count, cudaStream_t stream) {
+int registration_alloc(T** p, size_t count, RegistrationCache& cache, cudaStream_t stream) {
     *p = nullptr;
     if (count == 0) return kOk;
+    const size_t bytes = sizeof(T) * count;
+    if (void* q = cache.take(bytes)) {
+        *p = static_cast<T*>(q);
+        cache.registered(bytes, stream);
+        return kOk;
+    }
     cudaMemPool_t pool;
     int st = registration_pool(&pool);
     if (st != kOk) return st;
-    cudaError_t e = cudaMallocFromPoolAsync((void**)p, sizeof(T) * count, pool, stream);
+    cudaError_t e = cudaMallocFromPoolAsync((void**)p, bytes, pool, stream);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
         return check_cuda(e, "cudaMallocFromPoolAsync");
     }
+    cache.registered(bytes, stream);
     return kOk;
 }
 }  // namespace
@@ -276,8 +337,11 @@ struct ConfigState {
     Workspace cull;        // kept particles of the aliasing cull
     std::map<std::tuple<int, int, int>, cufftHandle> batched_plans;
     KernelTimer timer;
+    RegistrationCache registrations;  // blocks of unregistered datasets, for the next registration
 
     ~ConfigState() {
+        if (stream) cudaStreamSynchronize(stream);
+        registrations.release(stream);
         if (stream) cudaStreamSynchronize(stream);
         partials.release();
         arranged.release();
@@ -597,7 +661,7 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         }
         grp.d_number_of_terms = (int)padded;
         if (padded == 0) continue;
-        if (registration_alloc(&grp.d_constraints, (size_t)padded, s->stream) != kOk) return;
+        if (registration_alloc(&grp.d_constraints, (size_t)padded, s->registrations, s->stream) != kOk) return;
         cudaMemsetAsync(grp.d_constraints, 0, sizeof(Constraint) * padded, s->stream);
         cudaMemcpyAsync(grp.d_constraints, grp.h_constraints, sizeof(Constraint) * grp.number_of_terms,
                         cudaMemcpyHostToDevice, s->stream);
@@ -618,7 +682,7 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
             g_stats[grp.d_constraints] = gs;
         }
         if (grp.h_radii) {
-            if (registration_alloc(&grp.d_radii, (size_t)padded, s->stream) != kOk) return;
+            if (registration_alloc(&grp.d_radii, (size_t)padded, s->registrations, s->stream) != kOk) return;
             cudaMemsetAsync(grp.d_radii, 0, sizeof(float) * padded, s->stream);
             cudaMemcpyAsync(grp.d_radii, grp.h_radii, sizeof(float) * grp.number_of_terms, cudaMemcpyHostToDevice,
                             s->stream);
@@ -635,17 +699,21 @@ void vis_unregister_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         return;
     }
     // as cudaFree would: no launch on any stream still reads the arrays when
-    // their blocks go back to the pool
+    // their blocks go back to the config's cache (or the pool)
     cudaDeviceSynchronize();
     for (int g = 0; g < ds->number_of_groups; ++g) {
-        if (ds->groups[g].d_constraints) {
-            cudaFreeAsync(ds->groups[g].d_constraints, s->stream);
-            std::lock_guard<std::mutex> lock(g_stats_mu);
-            g_stats.erase(ds->groups[g].d_constraints);
+        Group& grp = ds->groups[g];
+        const size_t padded = (size_t)std::max(0, grp.d_number_of_terms);
+        if (grp.d_constraints) {
+            {
+                std::lock_guard<std::mutex> lock(g_stats_mu);
+                g_stats.erase(grp.d_constraints);
+            }
+            s->registrations.unregistered(grp.d_constraints, sizeof(Constraint) * padded, s->stream);
         }
-        if (ds->groups[g].d_radii) cudaFreeAsync(ds->groups[g].d_radii, s->stream);
-        ds->groups[g].d_constraints = nullptr;
-        ds->groups[g].d_radii = nullptr;
+        if (grp.d_radii) s->registrations.unregistered(grp.d_radii, sizeof(float) * padded, s->stream);
+        grp.d_constraints = nullptr;
+        grp.d_radii = nullptr;
     }
 }
 
@@ -1030,7 +1098,7 @@ struct VisBatch {
     Workspace partials, views_table;
     int n_views = 0;
     long long total_elements = 0;
-    std::vector<const void*> registered;  // device pointers the graph reads
+    std::vector<uint64_t> registered;  // batch_signature of the captured launches
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int mode = -1;  // -1 not built, 0 direct launches, 1 graph
@@ -1052,13 +1120,39 @@ struct VisBatch {
 
 namespace {
 
-std::vector<const void*> batch_pointers(const VisBatch* b) {
-    std::vector<const void*> out;
+// What a batch's captured launches depend on, per group: the device arrays,
+// the term count, and the registration statistics its plan reads (the weight
+// and radius extremes and the h-bin histogram).  An execute whose datasets
+// match the captured signature replays the graph; a frame registered at the
+// same addresses but with other statistics is planned and captured again.
+std::vector<uint64_t> batch_signature(const VisBatch* b) {
+    std::vector<uint64_t> out;
+    auto bits = [](float x) {
+        uint32_t u;
+        std::memcpy(&u, &x, sizeof u);
+        return (uint64_t)u;
+    };
     for (const VisBatch::Job& j : b->jobs)
         for (int g = 0; g < j.ds->number_of_groups; ++g) {
-            out.push_back(j.ds->groups[g].d_constraints);
-            out.push_back(j.ds->groups[g].d_radii);
-            out.push_back(reinterpret_cast<const void*>((intptr_t)j.ds->groups[g].number_of_terms));
+            const Group& grp = j.ds->groups[g];
+            out.push_back((uint64_t)(uintptr_t)grp.d_constraints);
+            out.push_back((uint64_t)(uintptr_t)grp.d_radii);
+            out.push_back((uint64_t)(uint32_t)grp.number_of_terms);
+            const GroupStats gs = registered_group_stats(grp.d_constraints);
+            out.push_back(bits(gs.radius_min) << 32 | bits(gs.radius_max));
+            out.push_back(bits(gs.weight_max));
+            uint64_t h = 1469598103934665603ull;  // FNV-1a of the histogram
+            if (gs.hbins) {
+                auto mix = [&h](const void* p, size_t n) {
+                    const unsigned char* c = static_cast<const unsigned char*>(p);
+                    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+                };
+                mix(&gs.hbins->h_min, sizeof(float));
+                mix(&gs.hbins->h_max, sizeof(float));
+                mix(gs.hbins->count.data(), gs.hbins->count.size() * sizeof(int));
+                mix(gs.hbins->wmax.data(), gs.hbins->wmax.size() * sizeof(float));
+            }
+            out.push_back(h);
         }
     return out;
 }
@@ -1198,7 +1292,7 @@ int batch_build(VisBatch* b, ConfigState* s, int form) {
         }
     }
     cudaGetLastError();
-    b->registered = batch_pointers(b);
+    b->registered = batch_signature(b);
     return kOk;
 }
 
@@ -1243,7 +1337,7 @@ int vis_batch_execute(VisBatch* b, int form) {
     ConfigState* s = b ? state_of(b->cfg) : nullptr;
     if (!s) return set_error(kInvalidValue, "vis_batch_execute: unknown batch");
     if (form < VIS_FORM_AUTO || form > VIS_FORM_TENSOR) return set_error(kInvalidValue, "vis_batch_execute: bad form");
-    if (b->mode < 0 || b->registered != batch_pointers(b)) return batch_build(b, s, form);
+    if (b->mode < 0 || b->registered != batch_signature(b)) return batch_build(b, s, form);
     if (b->mode == 1) return check_cuda(cudaGraphLaunch(b->exec, s->stream), "cudaGraphLaunch");
     return batch_enqueue(b, s);
 }

@@ -1594,6 +1594,7 @@ struct TcReduceArgs {
     bool factored;
     double scale;
     float2* out;
+    int warp_rows;  // planes: every warp sums all jobs of its own 32 rows (classes of fewer jobs than warps)
 };
 
 // Warps per block of the reduction kernels (each sums every eighth job).
@@ -1650,11 +1651,14 @@ __global__ void __launch_bounds__(32 * kReduceWarps) tc_reduce_kernel(TcReduceAr
     f.out[idx] = make_float2(o.x + (float)(tr * factor), o.y + (float)(ti * factor));
 }
 
-// The planes c < lz_tc of one output class, with the job list split over
-// warps: a block takes 32 rows (lanes) x kReduceC planes, warp w sums jobs w,
-// w + 8, ..., and the eight partial sums are added in warp order (a fixed
-// order: the result does not depend on timing), so eight independent load
-// chains per element hide the slots' latency.
+// The planes c < lz_tc of one output class.  With the job list split over
+// warps (classes of at least 8 jobs): a block takes 32 rows (lanes) x
+// kReduceC planes, warp w sums jobs w, w + 8, ..., and the eight partial sums
+// are added in warp order (a fixed order: the result does not depend on
+// timing), so eight independent load chains per element hide the slots'
+// latency.  With fewer jobs (f.warp_rows; one group per class, as in a batch
+// of particle sets) a block takes 8 x 32 rows and each warp sums every job of
+// its own 32 rows in job order, so no warp idles.
 __global__ void __launch_bounds__(32 * kReduceWarps, 2) tc_reduce_planes_kernel(TcReduceArgs f) {
     extern __shared__ __align__(16) unsigned char s_raw[];  // n_list descriptors, then the partial sums
     ReduceJob* s_jobs = reinterpret_cast<ReduceJob*>(s_raw);
@@ -1664,8 +1668,9 @@ __global__ void __launch_bounds__(32 * kReduceWarps, 2) tc_reduce_planes_kernel(
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long rows = (long long)f.kx * f.ky;
-    const long long row_blocks = (rows + 31) / 32;
-    const int rho = (int)((blockIdx.x % row_blocks) * 32 + lane);
+    const int block_rows = f.warp_rows ? 32 * kReduceWarps : 32;
+    const long long row_blocks = (rows + block_rows - 1) / block_rows;
+    const int rho = (int)((blockIdx.x % row_blocks) * block_rows + (f.warp_rows ? warp * 32 : 0) + lane);
     const int c0 = (int)(blockIdx.x / row_blocks) * kReduceC;
     const bool active = rho < rows;
     const int rr = active ? rho : 0;
@@ -1674,6 +1679,21 @@ __global__ void __launch_bounds__(32 * kReduceWarps, 2) tc_reduce_planes_kernel(
 #pragma unroll
     for (int i = 0; i < kReduceC; ++i) n2[i] = a * a + b * b + (c0 + i) * (c0 + i);
     double sr[kReduceC] = {}, si[kReduceC] = {};
+    // spectrum element (rho, c0 + i) += its FP64 sum, with the factored Phi^
+    auto store = [&](int i, double tr, double ti) {
+        double factor = f.scale;
+        if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[i]) * f.h);
+        const size_t idx = (size_t)rho * f.lz_out + c0 + i;
+        const float2 o = f.out[idx];
+        f.out[idx] = make_float2(o.x + (float)(tr * factor), o.y + (float)(ti * factor));
+    };
+    if (f.warp_rows) {  // uniform over the block: no barrier follows
+        if (!active) return;
+        for (int j = 0; j < f.n_list; ++j) reduce_add(s_jobs[j], rho, c0, n2, kReduceC, sr, si, 1.0);
+#pragma unroll
+        for (int i = 0; i < kReduceC; ++i) store(i, sr[i], si[i]);
+        return;
+    }
     if (active)
         for (int j = warp; j < f.n_list; j += kReduceWarps) reduce_add(s_jobs[j], rho, c0, n2, kReduceC, sr, si, 1.0);
 #pragma unroll
@@ -1688,11 +1708,7 @@ __global__ void __launch_bounds__(32 * kReduceWarps, 2) tc_reduce_planes_kernel(
             tr += v.x;
             ti += v.y;
         }
-        double factor = f.scale;
-        if (f.factored) factor *= phi_fp64(f.basis, f.step * sqrt((double)n2[i]) * f.h);
-        const size_t idx = (size_t)rho * f.lz_out + c0 + i;
-        const float2 o = f.out[idx];
-        f.out[idx] = make_float2(o.x + (float)(tr * factor), o.y + (float)(ti * factor));
+        store(i, tr, ti);
     }
 }
 
@@ -2745,8 +2761,11 @@ int tensor_enqueue(const std::vector<SumRequest>& groups, const TensorPlan& plan
         f.factored = c.factored;
         f.scale = c.scale;
         f.out = c.out;
+        f.warp_rows = f.n_list < kReduceWarps ? 1 : 0;
         if (f.n_list > 0) {
-            const long long blocks = ((long long)c.kx * c.ky + 31) / 32 * (c.lz_tc / kReduceC);
+            const int block_rows = f.warp_rows ? 32 * kReduceWarps : 32;
+            const long long blocks =
+                ((long long)c.kx * c.ky + block_rows - 1) / block_rows * (c.lz_tc / kReduceC);
             const size_t smem = (((size_t)f.n_list * sizeof(ReduceJob) + 15) & ~(size_t)15) +
                                 (size_t)kReduceWarps * 32 * kReduceC * sizeof(double2);
             st = reduce_smem(tc_reduce_planes_kernel, smem);

@@ -400,7 +400,8 @@ def test_batch_of_uneven_jobs_matches_fp64_and_replays_as_a_graph():
     """Three jobs of different particle counts, bases, lattices and image sizes
     (tensor-form and plain-form groups mixed) executed as one batch; each job's
     spectrum and views match the FP64 oracle, and a second execute replaying
-    the captured CUDA graph gives the same images."""
+    the captured CUDA graph gives the same images, also after the datasets are
+    unregistered and registered again."""
     rng = np.random.default_rng(41)
     cfg = M.Config(cutoff=(8, 8), samples=(16, 16), block_length=64)
     specs = [
@@ -435,6 +436,37 @@ def test_batch_of_uneven_jobs_matches_fp64_and_replays_as_a_graph():
         ref_imgs = O.render_from_spectrum(ref, grid, 1.0, (1.0, 1.0), cutoff, views, samples)
         assert O.rel_l2(imgs, ref_imgs) < IMAGE_TOL
         np.testing.assert_array_equal(imgs, first[j])
+    # a frame loop that registers the same datasets again gets the same device
+    # blocks back (the config keeps unregistered blocks for the next
+    # registration of the same size), so the batch replays its graph: no
+    # launch passes through the library's host code
+    addrs = [(ds.group(0).d_constraints, ds.group(0).d_radii) for ds in datasets]
+    lib = M.lib()
+    for _ in range(2):
+        for ds in datasets:
+            cfg.unregister(ds)
+        for ds in datasets:
+            cfg.register(ds)
+        assert [(ds.group(0).d_constraints, ds.group(0).d_radii) for ds in datasets] == addrs
+        c0 = lib.vis_kernel_launch_count()
+        batch.execute(M.FORM_AUTO)
+        assert lib.vis_kernel_launch_count() == c0 and batch.uses_graph() == 1
+        for j in range(len(specs)):
+            np.testing.assert_array_equal(batch.images(j), first[j])
+    # new weights at the same addresses change the registration statistics
+    # the plan reads (the weight scale), so the batch is planned and captured
+    # again; the sum is linear in the weights
+    cons0 = datasets[0]._keep[0]
+    cons0["weight"] *= 2.0
+    cfg.unregister(datasets[0])
+    cfg.register(datasets[0])
+    assert (datasets[0].group(0).d_constraints, datasets[0].group(0).d_radii) == addrs[0]
+    c0 = lib.vis_kernel_launch_count()
+    batch.execute(M.FORM_AUTO)
+    assert lib.vis_kernel_launch_count() > c0 and batch.uses_graph() == 1
+    assert O.rel_l2(batch.images(0), 2.0 * first[0]) < 1e-5
+    for j in range(1, len(specs)):
+        np.testing.assert_array_equal(batch.images(j), first[j])
     batch.close()
     for ds in datasets:
         cfg.unregister(ds)
