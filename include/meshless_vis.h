@@ -79,6 +79,10 @@ void vis_config_change_number_of_partial_sums(VisConfig* vis_config, int number_
 void vis_config_destroy(VisConfig* vis_config);
 void vis_config_compute_scale(VisConfig* vis_config);
 void vis_register_meshless_dataset(VisConfig* vis_config, MeshlessDataset* meshless_dataset);
+/* Unregistering synchronises the device and keeps the device blocks with the
+ * config for its next registration of the same byte size (so that a frame
+ * loop gets the same addresses back), up to the most the config had
+ * registered at once; vis_config_destroy releases them. */
 void vis_unregister_meshless_dataset(VisConfig* vis_config, MeshlessDataset* meshless_dataset);
 /* No graphics stack on the target: records VIS_ERROR_UNSUPPORTED and returns
  * without rendering.  Use vis_config_manual_d_image for a caller-owned device
