@@ -110,7 +110,6 @@ int hbin_fine_index(const std::vector<float>& edges, float h) {
 }
 
 namespace {
-std::atomic<unsigned long long> g_hbin_ids{0};
 
 // The smoothing-length histogram of a group whose Phi^ does not separate per
 // axis (SPH, WENDLAND_D3_C2) with varying radii; null otherwise.
@@ -129,7 +128,18 @@ std::shared_ptr<const HBinStats> hbin_histogram(const Group& grp, const GroupSta
         hs->count[f] += 1;
         hs->wmax[f] = std::max(hs->wmax[f], std::fabs(grp.h_constraints[k].weight));
     }
-    hs->id = g_hbin_ids.fetch_add(1) + 1;
+    // the id names the content (plans are cached by it): FNV-1a of the range,
+    // the counts and the weight maxima, never 0
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+    };
+    mix(&hs->h_min, sizeof(float));
+    mix(&hs->h_max, sizeof(float));
+    mix(hs->count.data(), hs->count.size() * sizeof(int));
+    mix(hs->wmax.data(), hs->wmax.size() * sizeof(float));
+    hs->id = h ? h : 1;
     return hs;
 }
 }  // namespace
@@ -1141,18 +1151,7 @@ std::vector<uint64_t> batch_signature(const VisBatch* b) {
             const GroupStats gs = registered_group_stats(grp.d_constraints);
             out.push_back(bits(gs.radius_min) << 32 | bits(gs.radius_max));
             out.push_back(bits(gs.weight_max));
-            uint64_t h = 1469598103934665603ull;  // FNV-1a of the histogram
-            if (gs.hbins) {
-                auto mix = [&h](const void* p, size_t n) {
-                    const unsigned char* c = static_cast<const unsigned char*>(p);
-                    for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
-                };
-                mix(&gs.hbins->h_min, sizeof(float));
-                mix(&gs.hbins->h_max, sizeof(float));
-                mix(gs.hbins->count.data(), gs.hbins->count.size() * sizeof(int));
-                mix(gs.hbins->wmax.data(), gs.hbins->wmax.size() * sizeof(float));
-            }
-            out.push_back(h);
+            out.push_back(gs.hbins ? gs.hbins->id : 0);  // the histogram's content hash
         }
     return out;
 }

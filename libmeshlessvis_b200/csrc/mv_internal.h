@@ -56,7 +56,7 @@ struct HBinStats {
     std::vector<float> edges;  // kHBinFine + 1
     std::vector<int> count;    // kHBinFine
     std::vector<float> wmax;   // kHBinFine
-    unsigned long long id = 0;  // unique per registration (cache key)
+    unsigned long long id = 0;  // hash of the content (plan cache key); equal data, equal id
 };
 std::vector<float> hbin_fine_edges(float h_min, float h_max);
 int hbin_fine_index(const std::vector<float>& edges, float h);

@@ -2501,7 +2501,9 @@ int tensor_prepare(const std::vector<SumRequest>& groups, TensorWorkspace& ws, c
     const size_t limit = operand_cache_limit();
     put(&limit, sizeof limit);
     for (const SumRequest& r : groups) {
-        const void* ptrs[6] = {r.particles, r.radii, r.out, r.hbins, r.shell_edges, r.shell_first};
+        // the histogram by its content id, not its address: a registration of
+        // the same data again gives the same plan
+        const void* ptrs[5] = {r.particles, r.radii, r.out, r.shell_edges, r.shell_first};
         put(ptrs, sizeof ptrs);
         const unsigned long long hid = r.hbins ? r.hbins->id : 0ull;
         put(&hid, sizeof hid);
