@@ -21,6 +21,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <unordered_map>
 #include <vector>
@@ -111,6 +112,37 @@ int hbin_fine_index(const std::vector<float>& edges, float h) {
 
 namespace {
 
+// Runs fn(part, begin, end) over [0, n) in contiguous ranges, one per host
+// thread (up to 16; the calling thread takes part 0), and returns the number
+// of parts.  Below 2^16 items, or when no thread can be started, one part
+// runs inline.  The registration's statistics are order-independent maxima,
+// minima and counts, so the parts' results combine to the serial ones.
+template <typename F>
+int parallel_parts(long long n, int max_parts, F fn) {
+    int parts = 1;
+    if (n >= (1LL << 16)) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        parts = (int)std::min<long long>(std::min<unsigned>(hw ? hw : 1, 16u), n >> 15);
+        parts = std::max(1, std::min(parts, max_parts));
+    }
+    std::vector<std::thread> threads;
+    int started = 1;
+    auto range = [&](int p) { return std::make_pair(n * p / parts, n * (p + 1) / parts); };
+    for (int p = 1; p < parts; ++p) {
+        try {
+            threads.emplace_back([&fn, p, range] { fn(p, range(p).first, range(p).second); });
+            ++started;
+        } catch (...) {
+            break;
+        }
+    }
+    // parts no thread took run here, after part 0
+    fn(0, range(0).first, range(0).second);
+    for (int p = started; p < parts; ++p) fn(p, range(p).first, range(p).second);
+    for (std::thread& t : threads) t.join();
+    return parts;
+}
+
 // hbin_fine_index for many radii against the same edges: a guess from the
 // logarithm, then float comparisons against the edges up and down to the
 // largest i with edges[i] <= h, so the result is the binary search's exactly
@@ -147,11 +179,23 @@ std::shared_ptr<const HBinStats> hbin_histogram(const Group& grp, const GroupSta
     hs->count.assign(kHBinFine, 0);
     hs->wmax.assign(kHBinFine, 0.f);
     const FineIndex fine(hs->edges);
-    for (int k = 0; k < grp.number_of_terms; ++k) {
-        const int f = fine(grp.h_radii[k]);
-        hs->count[f] += 1;
-        hs->wmax[f] = std::max(hs->wmax[f], std::fabs(grp.h_constraints[k].weight));
-    }
+    constexpr int kMaxParts = 16;
+    std::vector<std::vector<int>> count(kMaxParts);
+    std::vector<std::vector<float>> wmax(kMaxParts);
+    const int parts = parallel_parts(grp.number_of_terms, kMaxParts, [&](int p, long long b, long long e) {
+        count[p].assign(kHBinFine, 0);
+        wmax[p].assign(kHBinFine, 0.f);
+        for (long long k = b; k < e; ++k) {
+            const int f = fine(grp.h_radii[k]);
+            count[p][f] += 1;
+            wmax[p][f] = std::max(wmax[p][f], std::fabs(grp.h_constraints[k].weight));
+        }
+    });
+    for (int p = 0; p < parts; ++p)
+        for (int f = 0; f < kHBinFine; ++f) {
+            hs->count[f] += count[p][f];
+            hs->wmax[f] = std::max(hs->wmax[f], wmax[p][f]);
+        }
     // the id names the content (plans are cached by it): FNV-1a of the range,
     // the counts and the weight maxima, never 0
     uint64_t h = 1469598103934665603ull;
@@ -700,16 +744,36 @@ void vis_register_meshless_dataset(VisConfig* c, MeshlessDataset* ds) {
         cudaMemcpyAsync(grp.d_constraints, grp.h_constraints, sizeof(Constraint) * grp.number_of_terms,
                         cudaMemcpyHostToDevice, s->stream);
         GroupStats gs;
-        gs.weight_max = 0.f;
-        for (int k = 0; k < grp.number_of_terms; ++k)
-            gs.weight_max = std::max(gs.weight_max, std::fabs(grp.h_constraints[k].weight));
-        if (grp.h_radii && grp.number_of_terms > 0) {
-            gs.radius_min = gs.radius_max = grp.h_radii[0];
-            for (int k = 1; k < grp.number_of_terms; ++k) {
-                gs.radius_min = std::min(gs.radius_min, grp.h_radii[k]);
-                gs.radius_max = std::max(gs.radius_max, grp.h_radii[k]);
+        // the largest |weight| and the radius extremes: each part folds from
+        // the same start as the serial loop (0, and the first radius), so a
+        // NaN is ignored, or kept from the first radius, alike
+        {
+            constexpr int kMaxParts = 16;
+            const bool radii = grp.h_radii && grp.number_of_terms > 0;
+            const float r0 = radii ? grp.h_radii[0] : 0.f;
+            float wm[kMaxParts], rmin[kMaxParts], rmax[kMaxParts];
+            const int parts = parallel_parts(grp.number_of_terms, kMaxParts, [&](int p, long long b, long long e) {
+                float w = 0.f, lo = r0, hi = r0;
+                for (long long k = b; k < e; ++k) w = std::max(w, std::fabs(grp.h_constraints[k].weight));
+                if (radii)
+                    for (long long k = b; k < e; ++k) {
+                        lo = std::min(lo, grp.h_radii[k]);
+                        hi = std::max(hi, grp.h_radii[k]);
+                    }
+                wm[p] = w;
+                rmin[p] = lo;
+                rmax[p] = hi;
+            });
+            gs.weight_max = 0.f;
+            for (int p = 0; p < parts; ++p) gs.weight_max = std::max(gs.weight_max, wm[p]);
+            if (radii) {
+                gs.radius_min = gs.radius_max = r0;
+                for (int p = 0; p < parts; ++p) {
+                    gs.radius_min = std::min(gs.radius_min, rmin[p]);
+                    gs.radius_max = std::max(gs.radius_max, rmax[p]);
+                }
+                gs.hbins = hbin_histogram(grp, gs);
             }
-            gs.hbins = hbin_histogram(grp, gs);
         }
         {
             std::lock_guard<std::mutex> lock(g_stats_mu);
